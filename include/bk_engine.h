@@ -1,0 +1,108 @@
+/*
+ * bk_engine.h — C ABI of the B200 statevector engine for the transverse-field
+ * Trotter path of ssk1001/bernasconi-krylov.
+ *
+ * Plain C: no C++ or torch types cross this boundary. Every entry point returns
+ * a bk_status; human-readable detail for the last failure on a context is
+ * available from bk_last_error(). Citations name the reference interface each
+ * entry point replaces (paths relative to the reference project root).
+ */
+#ifndef BK_ENGINE_H
+#define BK_ENGINE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BK_ABI_VERSION 1
+
+typedef enum bk_status {
+  BK_OK = 0,
+  BK_ERR_INVALID = 1,     /* bad argument (n out of range, NaN field, NULL pointer, ...) */
+  BK_ERR_CUDA = 2,        /* CUDA runtime/driver error */
+  BK_ERR_OOM = 3,         /* device allocation failed or size overflow */
+  BK_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up (kernel returned early) */
+  BK_ERR_NORM = 5,        /* |psi|^2 left the tolerance band at a measured step */
+  BK_ERR_UNSUPPORTED = 6, /* configuration not provided by this build (e.g. n > 30) */
+  BK_ERR_NO_DEVICE = 7    /* no CUDA device / not an sm_100 device */
+} bk_status;
+
+typedef enum bk_precision { BK_C64 = 0, BK_C128 = 1 } bk_precision;
+
+/* BK_FUSED: tiled passes (diagonal phase + mixer + reductions fused, 64 KB tiles).
+ * BK_PLAIN: one diagonal-phase kernel then one 2x2 Rx kernel per qubit, the
+ *           launch structure of the reference's cuStateVec loop (sampler.cuh:604-618). */
+typedef enum bk_method { BK_FUSED = 0, BK_PLAIN = 1 } bk_method;
+
+/* BK_ORDER_REFERENCE: psi_k = (M D)^k psi_0, the reference's step (sampler.cuh:604-618).
+ * BK_ORDER_STRANG:    psi_k = (D^1/2 M D^1/2)^k psi_0. |psi|^2 — hence P_<, <d_H>,
+ *                     norms and samples — equals the reference ordering; only the
+ *                     exported amplitudes differ by the diagonal phase D^1/2. */
+typedef enum bk_ordering { BK_ORDER_REFERENCE = 0, BK_ORDER_STRANG = 1 } bk_ordering;
+
+typedef struct bk_ctx bk_ctx;
+
+/* Context = one device + one stream + cached device buffers (E table per n,
+ * statevector, reduction scratch). One context per host thread.
+ * Replaces CuStateVecSampler construction / destruction (sampler.cuh:402-410). */
+int bk_create(int device, bk_ctx** out);
+int bk_destroy(bk_ctx* ctx);
+const char* bk_last_error(const bk_ctx* ctx);
+const char* bk_status_string(int status);
+int bk_abi_version(void);
+
+/* ---- LABS energy core (labs_energy.hpp:121-132, sampler.cuh:54-70, 198-227) ---- */
+
+/* E(s) for `count` host states (exact integers). */
+int bk_labs_energy(int n, const uint64_t* states, int64_t count, int64_t* energies_out);
+
+/* Device E table for n (cached on ctx); optionally copied to host (2^n uint16). */
+int bk_energy_table(bk_ctx* ctx, int n, uint16_t* host_out);
+
+/* #{s : E(s) < e0} and p_blind = count / 2^n (sampler.cuh:383-399). */
+int bk_p_blind(bk_ctx* ctx, int n, int64_t e0, uint64_t* count_out, double* p_blind_out);
+
+/* ---- Evolution (sampler.cuh:428-438, 451-457, 509-619, 149-195) ---- */
+
+typedef struct bk_evolve_params {
+  int32_t n;           /* qubits, 1..30 */
+  int32_t precision;   /* bk_precision */
+  int32_t method;      /* bk_method */
+  int32_t ordering;    /* bk_ordering */
+  uint64_t s0;         /* trap bits (masked to n); psi_0 = |s0> */
+  int64_t e0;          /* P_< threshold: E(s) < e0; < 0 means E(s0) */
+  double dt;           /* Trotter step */
+  double diag_scale;   /* phase exp(-i dt diag_scale E); <= 0 means 1/n (the reference's dt/n) */
+  int32_t n_steps;     /* Trotter steps */
+  int32_t reserved0;
+  const double* g;     /* host, n_steps entries (piecewise-constant schedule), or NULL */
+  double g_const;      /* field used when g == NULL */
+  const uint8_t* measure; /* host, n_steps + 1 flags: measure BEFORE step k (k = n_steps: final) */
+  double norm_tol;     /* > 0: fail with BK_ERR_NORM when | |psi|^2 - 1 | > norm_tol at a measured step */
+} bk_evolve_params;
+
+/* Runs the whole schedule on the device and returns one row per flagged step:
+ * p_less[m], d_h[m], norm[m] (host arrays of length sum(measure); norm may be NULL). */
+int bk_evolve(bk_ctx* ctx, const bk_evolve_params* p, double* p_less, double* d_h, double* norm);
+
+/* Copies the statevector left by the last bk_evolve to host as interleaved
+ * (re, im) doubles, 2 * 2^n entries, in the requested ordering's convention. */
+int bk_export_state(bk_ctx* ctx, double* host_state_ri);
+
+/* Per-kernel device time of the last bk_evolve when timing is enabled
+ * (CUDA events around every launch): name, launches, total milliseconds. */
+int bk_set_kernel_timing(bk_ctx* ctx, int enabled);
+int bk_kernel_timing(bk_ctx* ctx, int index, const char** name, int64_t* launches, double* total_ms);
+
+/* ---- Projective sampling (sampler.cuh:459-487, 559-598) ---- */
+
+/* Samples `shots` basis states from |psi|^2 of the state left by the last
+ * bk_evolve: inverse CDF (FP64 prefix sums), results in random-number order. */
+int bk_sample(bk_ctx* ctx, const double* randnums, int64_t shots, uint64_t* out_states);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BK_ENGINE_H */
