@@ -1,0 +1,307 @@
+#!/usr/bin/env python3
+"""Benchmark: Trotter amplitude-steps per second of the transverse-field LABS
+evolution at N = 28 on B200 (complex64 fused engine), the reference sampler's
+headline configuration ("Large N": one deep trap from the lowest 1% of 4000
+seeded steepest descents, g = 0.35, dt = 0.02, P_< and <d_H> every 20 steps).
+
+One bench step = `--trotter` Trotter steps (default 100, i.e. 5 measurement
+intervals) run through bk_evolve from the trap state; K steps cover 2000
+Trotter steps at the defaults, the configuration's full run.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU (launched by torchrun, one rank per GPU): independent replicas, each
+rank evolves its own trap (seed 42 + rank); no collective on the data path
+(weak scaling). `value` = all ranks' amp-steps / the slowest rank's device time.
+
+`--impl reference` times the reference's own algorithm (phase kernel, then one
+2x2 Rx per qubit, complex128) as restated on the host CPU in oracle/ (the
+reference's cuStateVec code cannot be built here), all host threads, one
+Trotter step per bench step. Under torchrun only rank 0 runs it.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.join(ROOT, "bernasconi-krylov_b200")
+for _p in (ROOT, PKG_ROOT):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Trotter amp-steps/s at N={n}"
+UNIT = "amp-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=28)
+    ap.add_argument("--precision", choices=["c64", "c128"], default="c64")
+    ap.add_argument("--trotter", type=int, default=100, help="Trotter steps per bench step")
+    ap.add_argument("--measure-every", type=int, default=20)
+    ap.add_argument("--g", type=float, default=0.35)
+    ap.add_argument("--dt", type=float, default=0.02)
+    ap.add_argument("--cpu-baseline-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(n, steps, g, dt):
+    """The oracle's complex128 per-qubit restatement of the reference step, all host threads."""
+    from oracle import oracle as O
+    import bk_b200 as bk
+    bits, e0 = bk.select_trap(n, 42, 4000 if n >= 28 else 1000, 0.01 if n >= 28 else 0.05)
+    secs = np.zeros(steps)
+    threads = os.cpu_count() or 1
+    O.trotter_evolve(n, bits, e0, g, dt, steps, measure=[0], threads=threads, step_seconds=secs)
+    return {"value": (1 << n) / float(np.mean(secs)), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} Trotter steps of the N={n} trap in complex128 on the host "
+                      f"(oracle/trotter_oracle.cpp: phase + {n} per-qubit Rx passes per step, OpenMP), "
+                      f"mean step time {np.mean(secs):.3f} s"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    import bk_b200 as bk
+    n = a.n
+    bits, e0 = bk.select_trap(n, 42, 4000 if n >= 28 else 1000, 0.01 if n >= 28 else 0.05)
+    total = a.warmup + a.steps
+    secs = np.zeros(total)
+    threads = os.cpu_count() or 1
+    meas = [k for k in range(0, total + 1) if k % a.measure_every == 0]
+    O.trotter_evolve(n, bits, e0, a.g, a.dt, total, measure=meas, threads=threads, step_seconds=secs)
+    timed = secs[a.warmup:]
+    v = (1 << n) * len(timed) / float(timed.sum())
+    line = {"metric": METRIC.format(n=n), "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * float(timed.mean()),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic (seeded trap from 4000 steepest descents, no dataset)",
+            "config": {"workload": f"N={n} single trap, g={a.g}, dt={a.dt}, 1 Trotter step per bench step, "
+                                   f"P_< and <d_H> every {a.measure_every} steps", "n": n,
+                       "trap_bits": hex(bits), "trap_energy": e0},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{total} Trotter steps of the N={n} trap (oracle complex128 restatement of "
+                                       f"the reference's phase + per-qubit Rx loop), timed per step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+    import torch.distributed as dist
+    import bk_b200 as bk
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, T = a.n, a.trotter
+    prec = bk.BK_C64 if a.precision == "c64" else bk.BK_C128
+    eng = bk.Engine(local)
+    bits, e0 = bk.select_trap(n, 42 + rank, 4000, 0.01)
+    meas = list(range(0, T + 1, a.measure_every))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.ExternalStream(eng.stream_handle(), device=dev)
+
+    def bench_step():
+        return eng.evolve(n, bits, a.g, a.dt, T, measure=meas, e0=e0, precision=prec)
+
+    for _ in range(max(a.warmup, 0)):
+        bench_step()
+
+    # ---- device-timed region (value + live per-kernel timing) ----
+    barrier()
+    torch.cuda.synchronize(dev)
+    eng.set_kernel_timing(True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            p_last, d_last, n_last = bench_step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier()
+    dev_s = ev0.elapsed_time(ev1) / 1e3
+    timing = eng.kernel_timing()
+    eng.set_kernel_timing(False)
+    dev_s_max = max_over_ranks(dev_s)
+
+    # ---- end-to-end region: the C-ABI call with host buffers, wall clock ----
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        bench_step()
+    torch.cuda.synchronize(dev)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+
+    amp_steps = float(1 << n) * T * a.steps * world
+    value = amp_steps / dev_s_max
+    e2e = amp_steps / e2e_s
+
+    # ---- roofline of the dominant kernel ----
+    S = 8 if prec == bk.BK_C64 else 16
+    per_launch_bytes = {"a1_step": 2 * S, "a1_step_measure": 2 * S, "a1_measure": S, "measure": S,
+                        "plain_phase": 2 * S, "plain_rx": 2 * S}
+    dom = max(timing.items(), key=lambda kv: kv[1][1])
+    dname, (dl, dms) = dom
+    abytes = per_launch_bytes.get(dname, 2 * S) * float(1 << n)
+    achieved = abytes / (dms / dl / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = committed_traffic().get(f"{dname}/n{n}/{a.precision}")
+    launches = sum(v[0] for v in timing.values()) + a.steps  # + one basis-state init per call
+
+    line = {"metric": METRIC.format(n=n), "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * dev_s_max / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64" if prec == bk.BK_C64 else "c128",
+            "data": "synthetic (seeded trap from 4000 steepest descents, no dataset)",
+            "config": {"workload": f"N={n} single trap (lowest 1% of 4000 descents, seed {42 + rank}), g={a.g}, "
+                                   f"dt={a.dt}, {T} Trotter steps per bench step, P_< and <d_H> every "
+                                   f"{a.measure_every} steps, {a.precision} fused",
+                       "n": n, "trap_bits": hex(bits), "trap_energy": e0, "trotter_steps_per_step": T,
+                       "l2": f"state {((1 << n) * S) / 2**30:.1f} GiB > 126 MB L2, no flush needed",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": dms / dl,
+                         "traffic": traffic},
+            "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 3)} for k, v in timing.items()},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * 8 + (T + 1),
+                    "d2h_bytes_per_step": 8 * 3 * len(meas) + 8 * 4 * len(meas)},
+            "gpu_launches": launches, "clocks": clocks.summary(),
+            "check": {"p_less_last": float(p_last[-1]), "d_h_last": float(d_last[-1]),
+                      "norm_last": float(n_last[-1])}}
+
+    if rank == 0 and world == 1 and not a.no_compare:
+        cmp = {}
+        for name, pr, meth, steps in (("c128_fused", bk.BK_C128, bk.BK_FUSED, 40),
+                                      ("c128_plain", bk.BK_C128, bk.BK_PLAIN, 20)):
+            eng.evolve(n, bits, a.g, a.dt, 2, measure=[0], e0=e0, precision=pr, method=meth)
+            torch.cuda.synchronize(dev)
+            e0_ = torch.cuda.Event(enable_timing=True)
+            e1_ = torch.cuda.Event(enable_timing=True)
+            e0_.record(stream)
+            eng.evolve(n, bits, a.g, a.dt, steps, measure=list(range(0, steps + 1, a.measure_every)), e0=e0,
+                       precision=pr, method=meth)
+            e1_.record(stream)
+            torch.cuda.synchronize(dev)
+            cmp[name] = float(1 << n) * steps / (e0_.elapsed_time(e1_) / 1e3)
+        cmp["c64_fused"] = value
+        cmp["c64_fused_over_c128_plain"] = value / cmp["c128_plain"]
+        cmp["c64_fused_over_c128_fused"] = value / cmp["c128_fused"]
+        line["compare"] = cmp
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(n, a.cpu_baseline_steps, a.g, a.dt)
+        except Exception as exc:  # report, do not hide
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"failed: {exc}"}
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,331 @@
+// Auxiliary kernels: E table, p_blind count, state init, the whole-state kernel
+// for n <= T (all steps in one launch), the plain per-qubit path, state export
+// and projective sampling.
+#pragma once
+#include "bk_device.cuh"
+
+namespace bk {
+
+// E(s) for all s as uint16 (reference keeps doubles: src/sampling/sampler.cuh:54-70).
+// Each thread writes 8 consecutive states (one 16-byte store).
+__global__ void energy_table_kernel(uint16_t* __restrict__ out, int n, uint32_t count) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t s0 = g * 8u;
+  if (s0 >= count) return;
+  if (count - s0 >= 8u) {
+    uint16_t e[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) e[k] = (uint16_t)labs_energy(s0 + k, n);
+    uint4 q;
+    q.x = e[0] | ((uint32_t)e[1] << 16);
+    q.y = e[2] | ((uint32_t)e[3] << 16);
+    q.z = e[4] | ((uint32_t)e[5] << 16);
+    q.w = e[6] | ((uint32_t)e[7] << 16);
+    *reinterpret_cast<uint4*>(out + s0) = q;
+  } else {
+    for (uint32_t s = s0; s < count; ++s) out[s] = (uint16_t)labs_energy(s, n);
+  }
+}
+
+// #{s : E(s) < e0} (src/sampling/sampler.cuh:198-227); integer atomics are order-independent.
+__global__ void count_below_kernel(const uint16_t* __restrict__ E, uint32_t count, int e0,
+                                   unsigned long long* out) {
+  unsigned long long c = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    c += ((int)E[i] < e0) ? 1ull : 0ull;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+template <class A>
+__global__ void set_basis_kernel(A* psi, uint32_t idx) {
+  A one;
+  one.x = 1;
+  one.y = 0;
+  psi[idx] = one;
+}
+
+// ---------------------------------------------------------------------------
+// Whole-state kernel (n <= T): one CTA keeps the 2^n amplitudes in shared
+// memory and runs every step (measure if flagged, D, Rx on each qubit) in one
+// launch. Per-step tangents, D scale factors, measure flags and result slots
+// come from device arrays.
+// ---------------------------------------------------------------------------
+template <class R>
+struct SmallParams {
+  typename AmpTraits<R>::amp* state;
+  int n, n_steps;
+  const R* t;            // n_steps tangents
+  const R* amp_scale;    // n_steps exact powers of two folded into D
+  const int* slot;       // n_steps + 1: results row, or -1
+  const typename AmpTraits<R>::amp* phase_hi;
+  const typename AmpTraits<R>::amp* phase_lo;
+  int n_hi;
+  int e0;
+  uint32_t s0;
+  double* results;
+  int inverse;           // 1: apply the adjoint step (butterflies with -t, then conj(D))
+};
+
+template <class R>
+__global__ void __launch_bounds__(kThreads, 1) small_state_kernel(const SmallParams<R> p) {
+  using amp = typename AmpTraits<R>::amp;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int A = 1 << p.n;
+  amp* s = reinterpret_cast<amp*>(smem);
+  uint16_t* E = reinterpret_cast<uint16_t*>(smem + (size_t)A * sizeof(amp));
+  __shared__ double red[3][kThreads / 32];
+  for (int i = threadIdx.x; i < A; i += kThreads) {
+    s[i] = p.state[i];
+    E[i] = (uint16_t)labs_energy((uint32_t)i, p.n);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int step = 0; step <= p.n_steps; ++step) {
+    const int slot = p.slot[step];
+    if (slot >= 0) {
+      MeasureAcc acc;
+      for (int i = threadIdx.x; i < A; i += kThreads)
+        acc.add(norm2d(s[i]), (int)E[i] < p.e0, __popc((uint32_t)i ^ p.s0));
+      double a = warp_sum(acc.norm), b = warp_sum(acc.p_less), c = warp_sum(acc.d_h);
+      if (lane == 0) {
+        red[0][warp] = a;
+        red[1][warp] = b;
+        red[2][warp] = c;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double x = 0, y = 0, z = 0;
+        for (int w = 0; w < kThreads / 32; ++w) {
+          x += red[0][w];
+          y += red[1][w];
+          z += red[2][w];
+        }
+        p.results[4 * (size_t)slot + 0] = y;
+        p.results[4 * (size_t)slot + 1] = z;
+        p.results[4 * (size_t)slot + 2] = x;
+      }
+      __syncthreads();
+    }
+    if (step == p.n_steps) break;
+    const R t = p.inverse ? -p.t[step] : p.t[step];
+    if (!p.inverse) {
+      const R sc = p.amp_scale[step];
+      for (int i = threadIdx.x; i < A; i += kThreads) {
+        const int e = E[i];
+        amp h = p.phase_hi[e >> kPhaseLoBits];
+        h.x *= sc;
+        h.y *= sc;
+        s[i] = cmul(s[i], cmul(h, p.phase_lo[e & (kPhaseLo - 1)]));
+      }
+      __syncthreads();
+    }
+    for (int q = 0; q < p.n; ++q) {
+      for (int k = threadIdx.x; k < A / 2; k += kThreads) {
+        const int a = ((k >> q) << (q + 1)) | (k & ((1 << q) - 1));
+        bfly(s[a], s[a | (1 << q)], t);
+      }
+      __syncthreads();
+    }
+    if (p.inverse) {
+      const R sc = p.amp_scale[step];
+      for (int i = threadIdx.x; i < A; i += kThreads) {
+        const int e = E[i];
+        amp h = p.phase_hi[e >> kPhaseLoBits];
+        h.x *= sc;
+        h.y *= sc;
+        amp ph = cmul(h, p.phase_lo[e & (kPhaseLo - 1)]);
+        ph.y = -ph.y;
+        s[i] = cmul(s[i], ph);
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < A; i += kThreads) p.state[i] = s[i];
+}
+
+// ---------------------------------------------------------------------------
+// Plain path: the reference's launch structure (src/sampling/sampler.cuh:604-618)
+// — one diagonal-phase kernel per step with FP64 sincos (:73-91), then one
+// 2x2 kernel per qubit with the matrix [[c, i s], [i s, c]] (:451-457).
+// ---------------------------------------------------------------------------
+template <class A>
+__global__ void plain_phase_kernel(A* __restrict__ psi, const uint16_t* __restrict__ E, uint32_t count,
+                                   double dt_over_n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const double th = -dt_over_n * (double)E[i];
+  double sn, cs;
+  sincos(th, &sn, &cs);
+  const A a = psi[i];
+  A r;
+  r.x = (double)a.x * cs - (double)a.y * sn;
+  r.y = (double)a.x * sn + (double)a.y * cs;
+  psi[i] = r;
+}
+
+template <class A>
+__global__ void plain_rx_kernel(A* __restrict__ psi, uint32_t half, int q, double c, double s) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= half) return;
+  const uint32_t lo = k & ((1u << q) - 1u);
+  const uint32_t a = ((k >> q) << (q + 1)) | lo;
+  const uint32_t b = a | (1u << q);
+  const A x = psi[a], y = psi[b];
+  A xa, yb;
+  // [a'; b'] = [[c, i s], [i s, c]] [a; b]
+  xa.x = c * (double)x.x - s * (double)y.y;
+  xa.y = c * (double)x.y + s * (double)y.x;
+  yb.x = c * (double)y.x - s * (double)x.y;
+  yb.y = c * (double)y.y + s * (double)x.x;
+  psi[a] = xa;
+  psi[b] = yb;
+}
+
+// Measurement over the whole state (plain path and any state the tiled A1 pass
+// does not cover): fixed grid, FP64 per-block partials, ordered finalize.
+template <class A>
+__global__ void measure_kernel(const A* __restrict__ psi, const uint16_t* __restrict__ E, uint32_t count,
+                               int e0, uint32_t s0, double* partials, unsigned int* ticket, double* results,
+                               int slot) {
+  MeasureAcc acc;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    acc.add(norm2d(psi[i]), (int)E[i] < e0, __popc(i ^ s0));
+  block_reduce_and_finalize(acc, partials, ticket, results, slot, (int)gridDim.x);
+}
+
+// Export as interleaved (re, im) doubles, optionally multiplied by a diagonal
+// phase exp(-i angle_unit * E(s)) (Strang convention) and a real scale.
+template <class A>
+__global__ void export_kernel(const A* __restrict__ psi, const uint16_t* __restrict__ E, uint32_t count,
+                              double angle_unit, double scale, double2* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const A a = psi[i];
+  double2 r = make_double2((double)a.x * scale, (double)a.y * scale);
+  if (angle_unit != 0.0) {
+    double sn, cs;
+    sincos(-angle_unit * (double)E[i], &sn, &cs);
+    r = make_double2(r.x * cs - r.y * sn, r.x * sn + r.y * cs);
+  }
+  out[i] = r;
+}
+
+// ---------------------------------------------------------------------------
+// Projective sampling by inverse CDF (the reference calls the closed
+// custatevecSampler*, src/sampling/sampler.cuh:464-466, 564-573): chunk sums of
+// |psi|^2 in FP64, an exclusive scan over chunks, then per shot a binary search
+// over chunks and a warp scan inside the chunk. Shot k returns the smallest s
+// with u_k * total < cdf(s).
+// ---------------------------------------------------------------------------
+constexpr int kSampleChunkBits = 12;
+
+template <class A>
+__global__ void chunk_sums_kernel(const A* __restrict__ psi, uint32_t count, double* __restrict__ sums) {
+  const uint32_t chunk = blockIdx.x;
+  const uint32_t base = chunk << kSampleChunkBits;
+  const uint32_t len = min(1u << kSampleChunkBits, count - base);
+  double acc = 0.0;
+  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) acc += norm2d(psi[base + i]);
+  __shared__ double red[kThreads / 32];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) s += red[w];
+    sums[chunk] = s;
+  }
+}
+
+// In-place exclusive scan of `m` chunk sums by one block; total written to sums[m].
+__global__ void scan_chunks_kernel(double* sums, uint32_t m) {
+  __shared__ double carry;
+  __shared__ double wsum[32];
+  if (threadIdx.x == 0) carry = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t base = 0; base < m; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const double x = (i < m) ? sums[i] : 0.0;
+    double inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      double w = (lane < (int)(blockDim.x / 32)) ? wsum[lane] : 0.0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      wsum[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const double before = carry + (warp > 0 ? wsum[warp - 1] : 0.0);
+    if (i < m) sums[i] = before + inc - x;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = before + inc;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sums[m] = carry;
+}
+
+// One warp per shot.
+template <class A>
+__global__ void sample_kernel(const A* __restrict__ psi, uint32_t count, const double* __restrict__ prefix,
+                              uint32_t m, const double* __restrict__ randnums, int64_t shots,
+                              unsigned long long* __restrict__ out) {
+  const int64_t shot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (shot >= shots) return;
+  const double total = prefix[m];
+  const double target = randnums[shot] * total;
+  // last chunk whose exclusive prefix is <= target
+  uint32_t lo = 0, hi = m;  // answer in [lo, hi)
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (prefix[mid] <= target) lo = mid; else hi = mid;
+  }
+  const uint32_t base = lo << kSampleChunkBits;
+  const uint32_t len = min(1u << kSampleChunkBits, count - base);
+  const uint32_t per = (len + 31) / 32;
+  const uint32_t mine0 = min(len, lane * per), mine1 = min(len, mine0 + per);
+  double part = 0.0;
+  for (uint32_t i = mine0; i < mine1; ++i) part += norm2d(psi[base + i]);
+  double inc = part;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  const double start = prefix[lo] + inc - part;
+  const double end = prefix[lo] + inc;
+  // first lane whose inclusive cumulative exceeds the target
+  const unsigned ballot = __ballot_sync(0xffffffffu, target < end && mine1 > mine0);
+  uint32_t result = base + len - 1;  // rounding guard: clamp to the chunk's last state
+  if (ballot) {
+    const int owner = __ffs(ballot) - 1;
+    if (lane == owner) {
+      double c = start;
+      uint32_t r = mine1 - 1;
+      for (uint32_t i = mine0; i < mine1; ++i) {
+        c += norm2d(psi[base + i]);
+        if (target < c) {
+          r = i;
+          break;
+        }
+      }
+      out[shot] = base + r;
+    }
+  } else if (lane == 0) {
+    out[shot] = result;
+  }
+}
+
+}  // namespace bk

@@ -64,6 +64,25 @@ int bk_energy_table(bk_ctx* ctx, int n, uint16_t* host_out);
 /* #{s : E(s) < e0} and p_blind = count / 2^n (sampler.cuh:383-399). */
 int bk_p_blind(bk_ctx* ctx, int n, int64_t e0, uint64_t* count_out, double* p_blind_out);
 
+/* ---- Trap generation (classical.cuh:557-604, 625-712) ---- */
+
+/* ClassicalOptimizer(n, seed).random_state() drawn `count` times: mt19937_64(seed) & mask. */
+int bk_random_states(int n, uint64_t seed, int64_t count, uint64_t* out);
+
+/* Single-flip steepest descent from each start (first strictly best flip, lowest
+ * bit wins ties); max_evals = 0 means unlimited. Bit-exact with the reference's
+ * ClassicalOptimizer::steepest_descent. evals_out may be NULL. */
+int bk_steepest_descent(int n, const uint64_t* starts, int64_t count, uint64_t max_evals,
+                        uint64_t* final_states, int64_t* final_energies, uint64_t* evals_out);
+
+/* Trap selection used by the benchmark configurations: n_descents seeded
+ * descents (bk_random_states(n, seed) starts); among the local minima with
+ * E > E*(n) (not global optima), the threshold is the energy at `quantile` of
+ * their sorted energies, and the trap is the first minimum in generation order
+ * at or below it. */
+int bk_select_trap(int n, uint64_t seed, int32_t n_descents, double quantile, uint64_t* trap_bits,
+                   int64_t* trap_energy);
+
 /* ---- Evolution (sampler.cuh:428-438, 451-457, 509-619, 149-195) ---- */
 
 typedef struct bk_evolve_params {
@@ -95,6 +114,10 @@ int bk_export_state(bk_ctx* ctx, double* host_state_ri);
  * (CUDA events around every launch): name, launches, total milliseconds. */
 int bk_set_kernel_timing(bk_ctx* ctx, int enabled);
 int bk_kernel_timing(bk_ctx* ctx, int index, const char** name, int64_t* launches, double* total_ms);
+
+/* The context's CUDA stream (a cudaStream_t) so callers can order their own
+ * work and record CUDA events around the engine's launches. */
+int bk_stream(bk_ctx* ctx, void** stream_out);
 
 /* ---- Projective sampling (sampler.cuh:459-487, 559-598) ---- */
 

@@ -51,7 +51,7 @@ def lib():
         L.orc_steepest_descent.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, u64p, i64p, u64p, i64p]
         L.orc_trotter_evolve.restype = ctypes.c_int
         L.orc_trotter_evolve.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, dp, ctypes.c_double,
-                                         ctypes.c_double, ctypes.c_int, u8p, dp, dp, dp, ctypes.c_int, dp]
+                                         ctypes.c_double, ctypes.c_int, u8p, dp, dp, dp, ctypes.c_int, dp, dp]
         L.orc_sample_indices.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int64, u64p]
         L.orc_uniform_randoms.argtypes = [ctypes.c_uint64, ctypes.c_int64, dp]
         L.orc_sampler_run.restype = ctypes.c_int
@@ -129,8 +129,11 @@ def uniform_randoms(seed, count):
     return out
 
 
-def trotter_evolve(n, s0, e0, g, dt, n_steps, measure=None, diag_scale=0.0, threads=0, want_state=False):
-    """Complex128 restatement of the reference step loop; returns (p_less, d_h, norm[, state])."""
+def trotter_evolve(n, s0, e0, g, dt, n_steps, measure=None, diag_scale=0.0, threads=0, want_state=False,
+                   step_seconds=None):
+    """Complex128 restatement of the reference step loop; returns (p_less, d_h, norm[, state]).
+
+    ``step_seconds`` (optional float64 array of n_steps) receives the wall time of each step."""
     g_arr = np.ascontiguousarray(np.broadcast_to(np.asarray(g, dtype=np.float64), (max(n_steps, 1),)))
     if measure is None:
         flags = np.ones(n_steps + 1, dtype=np.uint8)
@@ -144,7 +147,8 @@ def trotter_evolve(n, s0, e0, g, dt, n_steps, measure=None, diag_scale=0.0, thre
     st = np.zeros(2 << n) if want_state else None
     rc = lib().orc_trotter_evolve(n, s0, e0, _ptr(g_arr, dp), dt, diag_scale, n_steps, _ptr(flags, u8p),
                                   _ptr(p, dp), _ptr(d, dp), _ptr(nn, dp), threads,
-                                  _ptr(st, dp) if want_state else None)
+                                  _ptr(st, dp) if want_state else None,
+                                  _ptr(step_seconds, dp) if step_seconds is not None else None)
     if rc != 0:
         raise ValueError(f"orc_trotter_evolve rejected n={n}, n_steps={n_steps}")
     if want_state:

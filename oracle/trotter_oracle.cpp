@@ -210,7 +210,8 @@ void orc_steepest_descent(int n, uint64_t start, uint64_t max_evals, uint64_t* f
 // ---------------------------------------------------------------------------
 int orc_trotter_evolve(int n, uint64_t s0, int64_t e0, const double* g_per_step, double dt,
                        double diag_scale, int n_steps, const uint8_t* measure, double* p_less,
-                       double* d_h, double* norm, int n_threads, double* state_out) {
+                       double* d_h, double* norm, int n_threads, double* state_out,
+                       double* step_seconds) {
   if (n < 1 || n > 30 || n_steps < 0) return 1;
 #ifdef _OPENMP
   if (n_threads > 0) omp_set_num_threads(n_threads);
@@ -226,6 +227,8 @@ int orc_trotter_evolve(int n, uint64_t s0, int64_t e0, const double* g_per_step,
 
   int mi = 0;
   for (int step = 0; step <= n_steps; ++step) {
+    // a step's wall time covers its measurement (if flagged) and the step itself
+    const double t_step0 = (step_seconds && step < n_steps) ? omp_get_wtime() : 0.0;
     if (measure == nullptr || measure[step]) {
       // fixed-order blocked reduction (deterministic for a given thread count)
       const int64_t nblk = std::min<int64_t>(A, 4096);
@@ -277,6 +280,7 @@ int orc_trotter_evolve(int n, uint64_t s0, int64_t e0, const double* g_per_step,
         psi[(size_t)b] = m01 * x + m00 * y;
       }
     }
+    if (step_seconds) step_seconds[step] = omp_get_wtime() - t_step0;
   }
   if (state_out) std::memcpy(state_out, psi.data(), sizeof(double) * 2 * (size_t)A);
   return 0;
