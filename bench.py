@@ -93,6 +93,12 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi's start-up can hold the driver for seconds; let it settle
+            # before the timed region so it cannot stall a timed launch
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 15:
+                time.sleep(0.05)
+            self.samples.clear()
         except Exception:
             self.proc = None
         return self

@@ -32,7 +32,39 @@ class EvolveParams(ctypes.Structure):
                 ("ordering", ctypes.c_int32), ("s0", ctypes.c_uint64), ("e0", ctypes.c_int64),
                 ("dt", ctypes.c_double), ("diag_scale", ctypes.c_double), ("n_steps", ctypes.c_int32),
                 ("reserved0", ctypes.c_int32), ("g", _dp), ("g_const", ctypes.c_double),
-                ("measure", _u8p), ("norm_tol", ctypes.c_double)]
+                ("measure", _u8p), ("norm_tol", ctypes.c_double), ("sample", _u8p), ("shots", ctypes.c_int32),
+                ("reserved1", ctypes.c_int32), ("randnums", _dp), ("samples_out", _u64p)]
+
+
+class SamplerConfigC(ctypes.Structure):
+    """bk_sampler_config — the reference's SamplerConfig (sampler.cuh:235-260) plus precision/method."""
+    _fields_ = [("n", ctypes.c_int32), ("num_sample_points", ctypes.c_int32), ("shots_per_point", ctypes.c_int32),
+                ("num_sampling_seeds", ctypes.c_int32), ("track_p_less", ctypes.c_int32),
+                ("record_trajectory", ctypes.c_int32), ("verbose", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("method", ctypes.c_int32), ("reserved", ctypes.c_int32), ("seed", ctypes.c_uint64),
+                ("seed_stride", ctypes.c_uint64), ("g", ctypes.c_double), ("dt", ctypes.c_double),
+                ("t_max", ctypes.c_double), ("t_start", ctypes.c_double), ("dt_sample", ctypes.c_double),
+                ("dt_trajectory", ctypes.c_double)]
+
+
+class SeedStatsC(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint64), ("total_shots_collected", ctypes.c_uint64),
+                ("improved_shots", ctypes.c_uint64), ("success_rate", ctypes.c_double),
+                ("per_eval_rate", ctypes.c_double), ("mean_hamming_flips", ctypes.c_double),
+                ("best_energy", ctypes.c_int64)]
+
+
+class SamplingResultC(ctypes.Structure):
+    _fields_ = [("unique_basis", _u64p), ("unique_basis_size", ctypes.c_int64),
+                ("total_shots_collected", ctypes.c_uint64), ("improved_shots", ctypes.c_uint64),
+                ("success_rate", ctypes.c_double), ("per_eval_rate", ctypes.c_double),
+                ("total_evals", ctypes.c_uint64), ("mean_hamming_flips", ctypes.c_double),
+                ("seed_stats", ctypes.POINTER(SeedStatsC)), ("n_seed_stats", ctypes.c_int32),
+                ("d_min", ctypes.c_int32), ("time_points", _dp), ("p_less_history", _dp), ("dh_history", _dp),
+                ("n_points", ctypes.c_int64), ("window_avg_dh", ctypes.c_double),
+                ("initial_rise_rate_avg", ctypes.c_double), ("initial_rise_rate_max", ctypes.c_double),
+                ("start_energy", ctypes.c_int64), ("p_blind", ctypes.c_double), ("peak_p_less", ctypes.c_double),
+                ("peak_time", ctypes.c_double)]
 
 
 def library_path():
@@ -69,6 +101,12 @@ def load_library(build_if_missing=True):
     L.bk_kernel_timing.argtypes = [c_ctx, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _i64p, _dp]
     L.bk_sample.argtypes = [c_ctx, _dp, ctypes.c_int64, _u64p]
     L.bk_stream.argtypes = [c_ctx, ctypes.POINTER(ctypes.c_void_p)]
+    L.bk_sampler_run.argtypes = [c_ctx, ctypes.POINTER(SamplerConfigC), ctypes.c_uint64,
+                                 ctypes.POINTER(SamplingResultC)]
+    L.bk_sampling_result_release.argtypes = [ctypes.POINTER(SamplingResultC)]
+    L.bk_sampling_result_release.restype = None
+    L.bk_d_min.argtypes = [c_ctx, ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int,
+                           ctypes.POINTER(ctypes.c_int)]
     L.bk_random_states.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, _u64p]
     L.bk_steepest_descent.argtypes = [ctypes.c_int, _u64p, ctypes.c_int64, ctypes.c_uint64, _u64p, _i64p, _u64p]
     L.bk_select_trap.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int32, ctypes.c_double, _u64p, _i64p]
@@ -191,6 +229,44 @@ class Engine:
         self._check(self.L.bk_evolve(self.ctx, ctypes.byref(gp), _p(p, _dp), _p(d, _dp), _p(nn, _dp)),
                     "bk_evolve")
         return p, d, nn
+
+    def d_min(self, n, bits, target=-1, max_d=-1):
+        d = ctypes.c_int()
+        self._check(self.L.bk_d_min(self.ctx, n, bits, target, max_d, ctypes.byref(d)), "bk_d_min")
+        return int(d.value)
+
+    def sampler_run(self, start_bits, precision=BK_C128, method=BK_FUSED, **cfg):
+        """The reference's ISampler::sample(start_state, SamplerConfig) as a dict.
+
+        ``cfg`` takes the SamplerConfig field names (sampler.cuh:235-260) with the
+        reference's defaults."""
+        defaults = dict(n=16, g=0.5, dt=0.05, t_max=60.0, num_sample_points=20, shots_per_point=100, seed=42,
+                        num_sampling_seeds=3, seed_stride=10007, t_start=0.0, dt_sample=0.0, track_p_less=True,
+                        verbose=True, record_trajectory=False, dt_trajectory=0.0)
+        unknown = set(cfg) - set(defaults)
+        if unknown:
+            raise TypeError(f"unknown SamplerConfig fields: {sorted(unknown)}")
+        defaults.update(cfg)
+        c = SamplerConfigC(**{k: (int(v) if isinstance(v, bool) else v) for k, v in defaults.items()},
+                           precision=precision, method=method)
+        r = SamplingResultC()
+        st = self.L.bk_sampler_run(self.ctx, ctypes.byref(c), start_bits, ctypes.byref(r))
+        try:
+            self._check(st, "bk_sampler_run")
+            npt = r.n_points
+            out = {k: getattr(r, k) for k, _ in SamplingResultC._fields_
+                   if k not in ("unique_basis", "seed_stats", "time_points", "p_less_history", "dh_history")}
+            out["time_points"] = np.ctypeslib.as_array(r.time_points, (npt,)).copy() if npt else np.zeros(0)
+            out["p_less_history"] = np.ctypeslib.as_array(r.p_less_history, (npt,)).copy() if npt else np.zeros(0)
+            out["dh_history"] = np.ctypeslib.as_array(r.dh_history, (npt,)).copy() if npt else np.zeros(0)
+            nu = r.unique_basis_size
+            out["unique_basis"] = np.ctypeslib.as_array(r.unique_basis, (nu,)).copy() if nu else np.zeros(0, np.uint64)
+            out["seed_stats"] = [{k: getattr(r.seed_stats[i], k) for k, _ in SeedStatsC._fields_}
+                                 for i in range(r.n_seed_stats)]
+            return out
+        finally:
+            if st == BK_OK:
+                self.L.bk_sampling_result_release(ctypes.byref(r))
 
     def export_state(self, n):
         out = np.empty(2 << n)

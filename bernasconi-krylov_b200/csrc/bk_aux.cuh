@@ -59,13 +59,12 @@ struct SmallParams {
   const R* t;            // n_steps tangents
   const R* amp_scale;    // n_steps exact powers of two folded into D
   const int* slot;       // n_steps + 1: results row, or -1
-  const typename AmpTraits<R>::amp* phase_hi;
-  const typename AmpTraits<R>::amp* phase_lo;
-  int n_hi;
+  typename PhaseOf<R>::params phase;
   int e0;
   uint32_t s0;
   double* results;
   int inverse;           // 1: apply the adjoint step (butterflies with -t, then conj(D))
+  int measure_last;      // measure the entry at step n_steps (else the caller does later)
 };
 
 template <class R>
@@ -74,7 +73,9 @@ __global__ void __launch_bounds__(kThreads, 1) small_state_kernel(const SmallPar
   extern __shared__ __align__(1024) unsigned char smem[];
   const int A = 1 << p.n;
   amp* s = reinterpret_cast<amp*>(smem);
-  uint16_t* E = reinterpret_cast<uint16_t*>(smem + (size_t)A * sizeof(amp));
+  const auto tabs = PhaseOf<R>::stage(p.phase, smem);
+  s = reinterpret_cast<amp*>(smem + PhaseOf<R>::kSmemBytes);
+  uint16_t* E = reinterpret_cast<uint16_t*>(smem + PhaseOf<R>::kSmemBytes + (size_t)A * sizeof(amp));
   __shared__ double red[3][kThreads / 32];
   for (int i = threadIdx.x; i < A; i += kThreads) {
     s[i] = p.state[i];
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(kThreads, 1) small_state_kernel(const SmallPar
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int step = 0; step <= p.n_steps; ++step) {
-    const int slot = p.slot[step];
+    const int slot = (step < p.n_steps || p.measure_last) ? p.slot[step] : -1;
     if (slot >= 0) {
       MeasureAcc acc;
       for (int i = threadIdx.x; i < A; i += kThreads)
@@ -114,10 +115,10 @@ __global__ void __launch_bounds__(kThreads, 1) small_state_kernel(const SmallPar
       const R sc = p.amp_scale[step];
       for (int i = threadIdx.x; i < A; i += kThreads) {
         const int e = E[i];
-        amp h = p.phase_hi[e >> kPhaseLoBits];
-        h.x *= sc;
-        h.y *= sc;
-        s[i] = cmul(s[i], cmul(h, p.phase_lo[e & (kPhaseLo - 1)]));
+        amp v = PhaseOf<R>::apply(s[i], e, p.phase, tabs);
+        v.x *= sc;
+        v.y *= sc;
+        s[i] = v;
       }
       __syncthreads();
     }
@@ -132,12 +133,10 @@ __global__ void __launch_bounds__(kThreads, 1) small_state_kernel(const SmallPar
       const R sc = p.amp_scale[step];
       for (int i = threadIdx.x; i < A; i += kThreads) {
         const int e = E[i];
-        amp h = p.phase_hi[e >> kPhaseLoBits];
-        h.x *= sc;
-        h.y *= sc;
-        amp ph = cmul(h, p.phase_lo[e & (kPhaseLo - 1)]);
-        ph.y = -ph.y;
-        s[i] = cmul(s[i], ph);
+        amp v = PhaseOf<R>::apply_inverse(s[i], e, p.phase, tabs);
+        v.x *= sc;
+        v.y *= sc;
+        s[i] = v;
       }
       __syncthreads();
     }
@@ -325,6 +324,35 @@ __global__ void sample_kernel(const A* __restrict__ psi, uint32_t count, const d
     }
   } else if (lane == 0) {
     out[shot] = result;
+  }
+}
+
+}  // namespace bk
+
+namespace bk {
+
+// ---------------------------------------------------------------------------
+// d_min (reference: src/labs_energy/labs_energy.hpp:175-207): is there a state
+// with E < target on the Hamming sphere of radius d around s? Each thread
+// unranks masks of weight d (combinatorial number system, colex order) in a
+// grid-stride loop; the first hit raises *found and the others stop early.
+// binom[c * 32 + k] = C(c, k) for c, k < 32.
+// ---------------------------------------------------------------------------
+__global__ void dmin_sphere_kernel(int n, uint32_t s, int target, int d, unsigned long long count,
+                                   const unsigned long long* __restrict__ binom, int* found) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long r = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; r < count; r += stride) {
+    if (*reinterpret_cast<volatile int*>(found)) return;
+    uint32_t mask = 0;
+    unsigned long long rem = r;
+    int c = n - 1;
+    for (int k = d; k >= 1; --k) {
+      while (binom[c * 32 + k] > rem) --c;
+      mask |= 1u << c;
+      rem -= binom[c * 32 + k];
+      --c;
+    }
+    if (labs_energy(s ^ mask, n) < target) atomicExch(found, 1);
   }
 }
 

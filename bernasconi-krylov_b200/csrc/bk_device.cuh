@@ -32,8 +32,6 @@ struct AmpTraits<double> {
 };
 
 constexpr int kThreads = 256;
-constexpr int kPhaseLoBits = 7;  // phase(E) = hi[E >> 7] * lo[E & 127]
-constexpr int kPhaseLo = 1 << kPhaseLoBits;
 
 __host__ __device__ constexpr uint32_t pdep(uint32_t v, uint32_t mask) {
   uint32_t r = 0;
@@ -136,6 +134,166 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
+// ---- diagonal phase exp(i theta E), theta = -dt * diag_scale ----
+// complex64: E = h K + l. The rotation by theta*l (|theta| (K-1) <= 1/2) takes
+// its shear coefficients from Maclaurin polynomials; the rotation by theta*h K
+// comes from a table of at most kPhaseH entries {a, b} (a bank row or two of
+// shared memory, so the data-dependent lookups do not conflict) plus an exact
+// quarter turn i^q. A rotation by r is applied as three shears (x += a y;
+// y += b x; x += a y with a = -tan(r/2), b = sin r): a shear has determinant
+// exactly 1 whatever the rounding of a and b, so no energy level gains or loses
+// norm systematically from step to step (a rounded (cos, sin) pair would).
+constexpr int kPhaseH = 256;  // table capacity (entries used: host choice, 16 typically)
+
+struct Phase32 {
+  const float2* hab;   // [n_h] {-tan(r_h / 2), sin r_h}
+  const int* hq;       // [n_h] quarter turns of level h
+  uint32_t K, M;       // h = umulhi(E, M) (exact for E <= Emax, checked on the host)
+  float theta, theta_lo;  // angle per unit of E (negative) as a float pair
+  int n_h;
+};
+
+__device__ __forceinline__ void shear_rotate(float& x, float& y, float a, float b) {
+  x = fmaf(a, y, x);
+  y = fmaf(b, x, y);
+  x = fmaf(a, y, x);
+}
+__device__ __forceinline__ void shear_unrotate(float& x, float& y, float a, float b) {
+  x = fmaf(-a, y, x);
+  y = fmaf(-b, x, y);
+  x = fmaf(-a, y, x);
+}
+// multiply by i^q (exact)
+__device__ __forceinline__ void quarter_turns(float& x, float& y, int q) {
+  const float x0 = x, y0 = y;
+  const bool odd = q & 1, neg = q & 2;
+  x = odd ? -y0 : x0;
+  y = odd ? x0 : y0;
+  if (neg) {
+    x = -x;
+    y = -y;
+  }
+}
+// Shear coefficients of a rotation by r, |r| <= 1/2: a = -tan(r/2), b = sin r
+// (Maclaurin series of tan to x^9 and sin to r^9; truncation < 2e-9 there).
+__device__ __forceinline__ void small_rotation(float r, float& a, float& b) {
+  const float x = 0.5f * r, x2 = x * x;
+  float t = fmaf(x2, 62.0f / 2835.0f, 17.0f / 315.0f);
+  t = fmaf(x2, t, 2.0f / 15.0f);
+  t = fmaf(x2, t, 1.0f / 3.0f);
+  t = fmaf(x2, t, 1.0f);
+  a = -x * t;
+  const float r2 = r * r;
+  float u = fmaf(r2, 1.0f / 362880.0f, -1.0f / 5040.0f);
+  u = fmaf(r2, u, 1.0f / 120.0f);
+  u = fmaf(r2, u, -1.0f / 6.0f);
+  u = fmaf(r2, u, 1.0f);
+  b = r * u;
+}
+// level split of E and the residual angle
+__device__ __forceinline__ float residual_angle(int e, const Phase32& P, uint32_t& h) {
+  h = __umulhi((uint32_t)e, P.M);
+  const uint32_t l = (uint32_t)e - h * P.K;
+  const float lf = __int_as_float(0x4B000000 | l) - 8388608.0f;  // exact for l < 2^23
+  return fmaf(lf, P.theta, lf * P.theta_lo);
+}
+__device__ __forceinline__ float2 apply_phase(float2 v, int e, const Phase32& P, const float2* hab, const int* hq) {
+  uint32_t h;
+  const float r = residual_angle(e, P, h);
+  float a, b;
+  small_rotation(r, a, b);
+  shear_rotate(v.x, v.y, a, b);
+  const float2 H = hab[h];
+  shear_rotate(v.x, v.y, H.x, H.y);
+  quarter_turns(v.x, v.y, hq[h]);
+  return v;
+}
+__device__ __forceinline__ float2 apply_phase_inverse(float2 v, int e, const Phase32& P, const float2* hab,
+                                                      const int* hq) {
+  uint32_t h;
+  const float r = residual_angle(e, P, h);
+  float a, b;
+  small_rotation(r, a, b);
+  quarter_turns(v.x, v.y, (4 - hq[h]) & 3);
+  const float2 H = hab[h];
+  shear_unrotate(v.x, v.y, H.x, H.y);
+  shear_unrotate(v.x, v.y, a, b);
+  return v;
+}
+
+// complex128: rounded FP64 (cos, sin) tables, E = 128 h + l, hi[h] * lo[l]
+// (gain per level ~1e-16 per step).
+constexpr int kPhaseLoBits = 7;
+constexpr int kPhaseLo = 1 << kPhaseLoBits;
+constexpr int kPhaseHi64 = 72;  // > (8555 >> 7) + 1 entries at n = 30
+struct Phase64 {
+  const double2* hi;  // [n_hi] (cos, sin) of theta * 128 h
+  const double2* lo;  // [128]  (cos, sin) of theta * l
+  int n_hi;
+};
+__device__ __forceinline__ double2 apply_phase(double2 v, int e, const Phase64&, const double2* hi,
+                                               const double2* lo) {
+  const double2 h = hi[e >> kPhaseLoBits], l = lo[e & (kPhaseLo - 1)];
+  const double c = fma(h.x, l.x, -h.y * l.y), s = fma(h.x, l.y, h.y * l.x);
+  return make_double2(fma(v.x, c, -v.y * s), fma(v.x, s, v.y * c));
+}
+__device__ __forceinline__ double2 apply_phase_inverse(double2 v, int e, const Phase64&, const double2* hi,
+                                                       const double2* lo) {
+  const double2 h = hi[e >> kPhaseLoBits], l = lo[e & (kPhaseLo - 1)];
+  const double c = fma(h.x, l.x, -h.y * l.y), s = fma(h.x, l.y, h.y * l.x);
+  return make_double2(fma(v.x, c, v.y * s), fma(-v.x, s, v.y * c));
+}
+
+// Per-precision phase parameters and their shared-memory staging.
+template <class R>
+struct PhaseOf;
+template <>
+struct PhaseOf<float> {
+  using params = Phase32;
+  static constexpr int kSmemBytes = kPhaseH * (int)(sizeof(float2) + sizeof(int));
+  struct Smem {
+    const float2* a;
+    const int* b;
+  };
+  __device__ static Smem stage(const Phase32& P, unsigned char* s) {
+    float2* hab = reinterpret_cast<float2*>(s);
+    int* hq = reinterpret_cast<int*>(hab + kPhaseH);
+    for (int i = threadIdx.x; i < P.n_h; i += blockDim.x) {
+      hab[i] = P.hab[i];
+      hq[i] = P.hq[i];
+    }
+    return Smem{hab, hq};
+  }
+  __device__ static float2 apply(float2 v, int e, const Phase32& P, const Smem& t) {
+    return apply_phase(v, e, P, t.a, t.b);
+  }
+  __device__ static float2 apply_inverse(float2 v, int e, const Phase32& P, const Smem& t) {
+    return apply_phase_inverse(v, e, P, t.a, t.b);
+  }
+};
+template <>
+struct PhaseOf<double> {
+  using params = Phase64;
+  static constexpr int kSmemBytes = (kPhaseHi64 + kPhaseLo) * (int)sizeof(double2);
+  struct Smem {
+    const double2* a;
+    const double2* b;
+  };
+  __device__ static Smem stage(const Phase64& P, unsigned char* s) {
+    double2* hi = reinterpret_cast<double2*>(s);
+    double2* lo = hi + kPhaseHi64;
+    for (int i = threadIdx.x; i < P.n_hi; i += blockDim.x) hi[i] = P.hi[i];
+    for (int i = threadIdx.x; i < kPhaseLo; i += blockDim.x) lo[i] = P.lo[i];
+    return Smem{hi, lo};
+  }
+  __device__ static double2 apply(double2 v, int e, const Phase64& P, const Smem& t) {
+    return apply_phase(v, e, P, t.a, t.b);
+  }
+  __device__ static double2 apply_inverse(double2 v, int e, const Phase64& P, const Smem& t) {
+    return apply_phase_inverse(v, e, P, t.a, t.b);
+  }
+};
+
 __device__ __forceinline__ double norm2d(float2 a) { return (double)fmaf(a.x, a.x, a.y * a.y); }
 __device__ __forceinline__ double norm2d(double2 a) { return fma(a.x, a.x, a.y * a.y); }
 

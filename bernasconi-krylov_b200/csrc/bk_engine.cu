@@ -11,9 +11,12 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <iomanip>
+#include <iostream>
 #include <map>
 #include <random>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 #include "bk_aux.cuh"
@@ -72,6 +75,12 @@ struct bk_ctx {
   size_t chunks_cap = 0;
   void* d_io = nullptr;
   size_t io_cap = 0;
+  double* d_rand = nullptr;  // in-run sampling: uniforms and drawn states
+  size_t rand_cap = 0;
+  unsigned long long* d_samples = nullptr;
+  size_t samples_cap = 0;
+  unsigned long long* d_binom = nullptr;
+  int* d_found = nullptr;
   // tensor maps, keyed by (state ptr, n, precision, pass)
   std::map<std::string, TmaDesc> tma;
   // last evolution (for export / sampling)
@@ -312,25 +321,67 @@ int ensure_state(bk_ctx* c, int n, int prec) {
   return BK_OK;
 }
 
-template <class R>
-int upload_phase_tables(bk_ctx* c, int n, double angle_unit, int* n_hi_out) {
-  using amp = typename AmpTraits<R>::amp;
+// Host side of the diagonal phase exp(-i angle_unit E).
+// complex64: E = h K + l; n_h table entries (the fewest in 16, 32, ..., 256 with
+// angle_unit (K - 1) <= 1/2 so the residual polynomials stay accurate);
+// h = umulhi(E, M) checked exact for every E <= Emax.
+int build_phase(bk_ctx* c, int n, double angle_unit, Phase32* P) {
+  const int emax = (n - 1) * n * (2 * n - 1) / 6;
+  int n_h = 16;
+  uint32_t K = 0;
+  for (;; n_h *= 2) {
+    if (n_h > kPhaseH)
+      return fail(c, BK_ERR_UNSUPPORTED, "phase angle per unit energy %g too large for the table", angle_unit);
+    K = (uint32_t)((emax + n_h) / n_h);  // ceil((emax + 1) / n_h)
+    if (std::fabs(angle_unit) * (double)(K - 1) <= 0.5) break;
+  }
+  const uint32_t M = (uint32_t)((((uint64_t)1 << 32) + K - 1) / K);
+  for (uint64_t e = 0; e <= (uint64_t)emax; ++e)
+    if (((e * M) >> 32) != e / K) return fail(c, BK_ERR_UNSUPPORTED, "no exact level split for n = %d", n);
+  std::vector<float2> hab((size_t)n_h);
+  std::vector<int> hq((size_t)n_h);
+  const double half_pi = 1.5707963267948966;
+  for (int h = 0; h < n_h; ++h) {
+    const double th = -angle_unit * (double)h * (double)K;
+    const double q = std::nearbyint(th / half_pi);
+    const double r = th - q * half_pi;  // |r| <= pi/4
+    hab[(size_t)h] = make_float2((float)(-std::tan(0.5 * r)), (float)std::sin(r));
+    hq[(size_t)h] = (int)(((long long)std::fmod(q, 4.0) + 4) % 4);
+  }
+  const size_t b1 = hab.size() * sizeof(float2), b2 = hq.size() * sizeof(int);
+  BK_TRY(ensure_buffer(c, &c->d_phase, &c->phase_cap, b1 + b2));
+  BK_CUDA(c, cudaMemcpyAsync(c->d_phase, hab.data(), b1, cudaMemcpyHostToDevice, c->stream));
+  BK_CUDA(c, cudaMemcpyAsync(static_cast<char*>(c->d_phase) + b1, hq.data(), b2, cudaMemcpyHostToDevice, c->stream));
+  BK_CUDA(c, cudaStreamSynchronize(c->stream));  // host vectors die at return
+  P->hab = reinterpret_cast<const float2*>(c->d_phase);
+  P->hq = reinterpret_cast<const int*>(static_cast<char*>(c->d_phase) + b1);
+  P->K = K;
+  P->M = M;
+  P->theta = (float)(-angle_unit);
+  P->theta_lo = (float)(-angle_unit - (double)P->theta);
+  P->n_h = n_h;
+  return BK_OK;
+}
+// complex128: E = 128 h + l, FP64 (cos, sin) tables.
+int build_phase(bk_ctx* c, int n, double angle_unit, Phase64* P) {
   const int emax = (n - 1) * n * (2 * n - 1) / 6;
   const int n_hi = (emax >> kPhaseLoBits) + 1;
-  std::vector<amp> h((size_t)n_hi + kPhaseLo);
-  for (int i = 0; i < n_hi; ++i) {
-    const double th = -angle_unit * (double)(i << kPhaseLoBits);
-    h[(size_t)i].x = (R)std::cos(th);
-    h[(size_t)i].y = (R)std::sin(th);
+  if (n_hi > kPhaseHi64) return fail(c, BK_ERR_UNSUPPORTED, "n = %d exceeds the phase table", n);
+  std::vector<double2> t((size_t)n_hi + kPhaseLo);
+  for (int h = 0; h < n_hi; ++h) {
+    const double th = -angle_unit * (double)(h << kPhaseLoBits);
+    t[(size_t)h] = make_double2(std::cos(th), std::sin(th));
   }
-  for (int i = 0; i < kPhaseLo; ++i) {
-    const double th = -angle_unit * (double)i;
-    h[(size_t)n_hi + i].x = (R)std::cos(th);
-    h[(size_t)n_hi + i].y = (R)std::sin(th);
+  for (int l = 0; l < kPhaseLo; ++l) {
+    const double th = -angle_unit * (double)l;
+    t[(size_t)n_hi + l] = make_double2(std::cos(th), std::sin(th));
   }
-  BK_TRY(ensure_buffer(c, &c->d_phase, &c->phase_cap, h.size() * sizeof(amp)));
-  BK_CUDA(c, cudaMemcpyAsync(c->d_phase, h.data(), h.size() * sizeof(amp), cudaMemcpyHostToDevice, c->stream));
-  *n_hi_out = n_hi;
+  BK_TRY(ensure_buffer(c, &c->d_phase, &c->phase_cap, t.size() * sizeof(double2)));
+  BK_CUDA(c, cudaMemcpyAsync(c->d_phase, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  BK_CUDA(c, cudaStreamSynchronize(c->stream));
+  P->hi = reinterpret_cast<const double2*>(c->d_phase);
+  P->lo = P->hi + n_hi;
+  P->n_hi = n_hi;
   return BK_OK;
 }
 
@@ -340,7 +391,28 @@ struct Schedule {
   std::vector<double> g;        // per step
   std::vector<int> slot;        // per step (n_steps + 1): measurement row or -1
   int n_meas = 0;
+  std::vector<int> sample_pt;   // per step (n_steps + 1): sampling point index or -1
+  int n_pts = 0;
+  int shots = 0;
 };
+
+// Projective sampling of the current state at sampling point `pt`: chunk sums
+// of |psi|^2, exclusive scan, one warp per draw.
+template <class A>
+int launch_sampling(bk_ctx* c, const A* psi, int n, int pt, int shots) {
+  const uint32_t count = 1u << n;
+  const uint32_t m = (count + (1u << kSampleChunkBits) - 1) >> kSampleChunkBits;
+  BK_TRY(ensure_buffer(c, reinterpret_cast<void**>(&c->d_chunks), &c->chunks_cap, (m + 1) * sizeof(double)));
+  size_t ev = 0;
+  BK_TRY(ev_begin(c, "sample", &ev));
+  chunk_sums_kernel<A><<<m, 256, 0, c->stream>>>(psi, count, c->d_chunks);
+  scan_chunks_kernel<<<1, 1024, 0, c->stream>>>(c->d_chunks, m);
+  const unsigned blocks = (unsigned)(((size_t)shots * 32 + 255) / 256);
+  sample_kernel<A><<<blocks, 256, 0, c->stream>>>(psi, count, c->d_chunks, m, c->d_rand + (size_t)pt * shots,
+                                                  shots, c->d_samples + (size_t)pt * shots);
+  BK_CUDA(c, cudaGetLastError());
+  return ev_end(c, ev);
+}
 
 template <class R>
 int launch_a1(bk_ctx* c, int kind, const PassParams<R>& pp, const TmaDesc* am, const TmaDesc* em, int n) {
@@ -401,10 +473,8 @@ int evolve_fused(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
   constexpr int T = AmpTraits<R>::kTileBits;
   const int n = p->n;
   const double dt = p->dt;
-  int n_hi = 0;
-  BK_TRY(upload_phase_tables<R>(c, n, angle_unit, &n_hi));
-  const amp* ph_hi = reinterpret_cast<const amp*>(c->d_phase);
-  const amp* ph_lo = ph_hi + n_hi;
+  typename PhaseOf<R>::params phase{};
+  BK_TRY(build_phase(c, n, angle_unit, &phase));
   const int e0 = (int)p->e0;
   const uint32_t s0 = (uint32_t)(p->s0 & ((1ull << n) - 1ull));
 
@@ -423,13 +493,16 @@ int evolve_fused(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
       lg -= (long double)kRescaleLog2;
     }
     scales[(size_t)k] = sc;
-    lg += -(long double)n * std::log2(std::fabs((long double)std::cos((long double)gd)));
+    // each butterfly multiplies the norm^2 of its pair by 1 + t^2, t the value the kernel uses
+    const long double tf = (long double)tans[(size_t)k];
+    lg += 0.5L * (long double)n * std::log2(1.0L + tf * tf);
   }
   *final_log2 = lg;
 
   if (n <= T) {
-    // whole state in one CTA's shared memory; all steps in one launch
-    const size_t smem = (1ull << n) * (sizeof(amp) + 2);
+    // whole state in one CTA's shared memory; all steps between two sampling
+    // points in one launch
+    const size_t smem = PhaseOf<R>::kSmemBytes + (1ull << n) * (sizeof(amp) + 2);
     const size_t bytes = tans.size() * sizeof(R) * 2 + S.slot.size() * sizeof(int) + 64;
     BK_TRY(ensure_buffer(c, &c->d_small, &c->small_cap, bytes));
     char* base = reinterpret_cast<char*>(c->d_small);
@@ -441,27 +514,57 @@ int evolve_fused(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
       BK_CUDA(c, cudaMemcpyAsync(d_sc, scales.data(), scales.size() * sizeof(R), cudaMemcpyHostToDevice, c->stream));
     }
     BK_CUDA(c, cudaMemcpyAsync(d_slot, S.slot.data(), S.slot.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    SmallParams<R> sp;
-    sp.state = reinterpret_cast<amp*>(c->d_state);
-    sp.n = n;
-    sp.n_steps = p->n_steps;
-    sp.t = d_t;
-    sp.amp_scale = d_sc;
-    sp.slot = d_slot;
-    sp.phase_hi = ph_hi;
-    sp.phase_lo = ph_lo;
-    sp.n_hi = n_hi;
-    sp.e0 = e0;
-    sp.s0 = s0;
-    sp.results = c->d_results;
-    sp.inverse = 0;
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(small_state_kernel<R>),
-                      (int)((1ull << T) * (sizeof(amp) + 2))));
-    size_t ev = 0;
-    BK_TRY(ev_begin(c, "small_state", &ev));
-    small_state_kernel<R><<<1, kThreads, smem, c->stream>>>(sp);
-    BK_CUDA(c, cudaGetLastError());
-    return ev_end(c, ev);
+                      (int)(PhaseOf<R>::kSmemBytes + (1ull << T) * (sizeof(amp) + 2))));
+    // Segments end at sampling points: sampling reads psi_k before step k, so a
+    // segment runs steps [k0, k1) and leaves the measurement of step k1 to the
+    // next segment (measure_last = 0); the last segment measures its end.
+    int k0 = 0, search = 0;
+    while (true) {
+      int k1 = search;
+      while (k1 <= p->n_steps && S.sample_pt[(size_t)k1] < 0) ++k1;
+      const bool sample_here = (k1 <= p->n_steps);
+      SmallParams<R> sp;
+      sp.state = reinterpret_cast<amp*>(c->d_state);
+      sp.n = n;
+      sp.n_steps = (sample_here ? k1 : p->n_steps) - k0;
+      sp.t = d_t + k0;
+      sp.amp_scale = d_sc + k0;
+      sp.slot = d_slot + k0;
+      sp.phase = phase;
+      sp.e0 = e0;
+      sp.s0 = s0;
+      sp.results = c->d_results;
+      sp.inverse = 0;
+      sp.measure_last = sample_here ? 0 : 1;
+      if (sp.n_steps > 0 || sp.measure_last) {
+        size_t ev = 0;
+        BK_TRY(ev_begin(c, "small_state", &ev));
+        small_state_kernel<R><<<1, kThreads, smem, c->stream>>>(sp);
+        BK_CUDA(c, cudaGetLastError());
+        BK_TRY(ev_end(c, ev));
+      }
+      if (!sample_here) break;
+      BK_TRY(launch_sampling<amp>(c, reinterpret_cast<amp*>(c->d_state), n, S.sample_pt[(size_t)k1], S.shots));
+      k0 = k1;
+      search = k1 + 1;
+      if (k1 == p->n_steps) {
+        // sampling at the final step; its measurement follows in a zero-step launch
+        SmallParams<R> fp = sp;
+        fp.n_steps = 0;
+        fp.t = d_t;
+        fp.amp_scale = d_sc;
+        fp.slot = d_slot + k1;
+        fp.measure_last = 1;
+        size_t ev = 0;
+        BK_TRY(ev_begin(c, "small_state", &ev));
+        small_state_kernel<R><<<1, kThreads, smem, c->stream>>>(fp);
+        BK_CUDA(c, cudaGetLastError());
+        BK_TRY(ev_end(c, ev));
+        break;
+      }
+    }
+    return BK_OK;
   }
 
   // tiled passes
@@ -478,9 +581,7 @@ int evolve_fused(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
   PassParams<R> base{};
   base.state = reinterpret_cast<amp*>(c->d_state);
   base.n = (uint32_t)n;
-  base.phase_hi = ph_hi;
-  base.phase_lo = ph_lo;
-  base.n_hi = n_hi;
+  base.phase = phase;
   base.e0 = e0;
   base.s0 = s0;
   base.partials = c->d_partials;
@@ -492,6 +593,8 @@ int evolve_fused(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
 
   for (int k = 0; k <= p->n_steps; ++k) {
     const int slot = S.slot[(size_t)k];
+    if (S.sample_pt[(size_t)k] >= 0)
+      BK_TRY(launch_sampling<amp>(c, base.state, n, S.sample_pt[(size_t)k], S.shots));
     if (k == p->n_steps) {
       if (slot >= 0) {
         PassParams<R> pp = base;
@@ -540,6 +643,7 @@ int evolve_plain(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
   const unsigned th = 256;
   for (int k = 0; k <= p->n_steps; ++k) {
     const int slot = S.slot[(size_t)k];
+    if (S.sample_pt[(size_t)k] >= 0) BK_TRY(launch_sampling<amp>(c, psi, n, S.sample_pt[(size_t)k], S.shots));
     if (slot >= 0) {
       size_t ev = 0;
       BK_TRY(ev_begin(c, "measure", &ev));
@@ -699,7 +803,8 @@ int bk_destroy(bk_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (void* p : {(void*)c->d_E, c->d_state, (void*)c->d_partials, (void*)c->d_results, (void*)c->d_ticket,
-                  (void*)c->d_err, (void*)c->d_count, c->d_phase, c->d_small, (void*)c->d_chunks, c->d_io})
+                  (void*)c->d_err, (void*)c->d_count, c->d_phase, c->d_small, (void*)c->d_chunks, c->d_io,
+                  (void*)c->d_rand, (void*)c->d_samples, (void*)c->d_binom, (void*)c->d_found})
     if (p) cudaFree(p);
   for (auto& e : c->ev_pool) {
     cudaEventDestroy(e.first);
@@ -834,6 +939,14 @@ int bk_evolve(bk_ctx* c, const bk_evolve_params* p, double* p_less, double* d_h,
   for (int k = 0; k <= p->n_steps; ++k)
     if (p->measure == nullptr || p->measure[k]) S.slot[(size_t)k] = S.n_meas++;
   if (S.n_meas > 0 && (!p_less || !d_h)) return fail(c, BK_ERR_INVALID, "output arrays are NULL");
+  S.sample_pt.assign((size_t)p->n_steps + 1, -1);
+  if (p->sample != nullptr) {
+    if (p->shots <= 0 || !p->randnums || !p->samples_out)
+      return fail(c, BK_ERR_INVALID, "sampling needs shots > 0, randnums and samples_out");
+    for (int k = 0; k <= p->n_steps; ++k)
+      if (p->sample[k]) S.sample_pt[(size_t)k] = S.n_pts++;
+    S.shots = p->shots;
+  }
 
   int64_t e0 = p->e0;
   if (e0 < 0) BK_TRY(bk_labs_energy(n, &p->s0, 1, &e0));
@@ -850,6 +963,12 @@ int bk_evolve(bk_ctx* c, const bk_evolve_params* p, double* p_less, double* d_h,
                        3 * std::max<size_t>(grid, kMeasureGrid) * sizeof(double)));
   BK_TRY(ensure_buffer(c, reinterpret_cast<void**>(&c->d_results), &c->results_cap,
                        4 * std::max<size_t>((size_t)S.n_meas, 1) * sizeof(double)));
+  if (S.n_pts > 0) {
+    const size_t draws = (size_t)S.n_pts * (size_t)S.shots;
+    BK_TRY(ensure_buffer(c, reinterpret_cast<void**>(&c->d_rand), &c->rand_cap, draws * sizeof(double)));
+    BK_TRY(ensure_buffer(c, reinterpret_cast<void**>(&c->d_samples), &c->samples_cap, draws * sizeof(uint64_t)));
+    BK_CUDA(c, cudaMemcpyAsync(c->d_rand, p->randnums, draws * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
   BK_CUDA(c, cudaMemsetAsync(c->d_ticket, 0, sizeof(unsigned int), c->stream));
   BK_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
   BK_CUDA(c, cudaMemsetAsync(c->d_state, 0, (1ull << n) * amp_bytes(p->precision), c->stream));
@@ -878,6 +997,9 @@ int bk_evolve(bk_ctx* c, const bk_evolve_params* p, double* p_less, double* d_h,
   if (S.n_meas > 0)
     BK_CUDA(c, cudaMemcpyAsync(rows.data(), c->d_results, rows.size() * sizeof(double), cudaMemcpyDeviceToHost,
                                c->stream));
+  if (S.n_pts > 0)
+    BK_CUDA(c, cudaMemcpyAsync(p->samples_out, c->d_samples, (size_t)S.n_pts * S.shots * sizeof(uint64_t),
+                               cudaMemcpyDeviceToHost, c->stream));
   BK_TRY(check_device_error(c));
   BK_TRY(collect_timing(c));
   c->have_state = true;
@@ -896,6 +1018,295 @@ int bk_evolve(bk_ctx* c, const bk_evolve_params* p, double* p_less, double* d_h,
     if (p->norm_tol > 0.0 && !(std::fabs(nn - 1.0) <= p->norm_tol)) status = BK_ERR_NORM;
   }
   if (status == BK_ERR_NORM) return fail(c, BK_ERR_NORM, "norm left the tolerance band %g", p->norm_tol);
+  return BK_OK;
+}
+
+int bk_d_min(bk_ctx* c, int n, uint64_t bits, int64_t target, int max_d, int* d_out) {
+  if (!c || !d_out) return BK_ERR_INVALID;
+  if (n < 1 || n > kMaxN) return fail(c, BK_ERR_UNSUPPORTED, "n = %d outside [1, %d]", n, kMaxN);
+  const uint64_t m = (1ull << n) - 1ull;
+  const uint64_t sb = bits & m;
+  if (target < 0) target = host_energy(n, sb);
+  const int not_found = (max_d > 0) ? (max_d + 1) : n;
+  const int64_t opt = optimal_energy(n);
+  if (opt >= 0 && target <= opt) {
+    *d_out = not_found;
+    return BK_OK;
+  }
+  BK_CUDA(c, cudaSetDevice(c->device));
+  if (!c->d_binom) {
+    std::vector<unsigned long long> b(32 * 32, 0ull);
+    for (int i = 0; i < 32; ++i) {
+      b[(size_t)i * 32] = 1;
+      for (int k = 1; k <= i; ++k) b[(size_t)i * 32 + k] = b[(size_t)(i - 1) * 32 + k - 1] + (k < i ? b[(size_t)(i - 1) * 32 + k] : 0);
+    }
+    BK_CUDA(c, cudaMalloc(&c->d_binom, b.size() * sizeof(unsigned long long)));
+    BK_CUDA(c, cudaMalloc(&c->d_found, sizeof(int)));
+    BK_CUDA(c, cudaMemcpy(c->d_binom, b.data(), b.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+  }
+  const int limit = (max_d > 0 && max_d <= n) ? max_d : n;
+  for (int d = 1; d <= limit; ++d) {
+    if (d == n) {  // the full flip is the only weight-n mask
+      *d_out = (host_energy(n, sb ^ m) < target) ? n : not_found;
+      return BK_OK;
+    }
+    unsigned long long count = 1;
+    for (int k = 1; k <= d; ++k) count = count * (unsigned long long)(n - d + k) / (unsigned long long)k;
+    BK_CUDA(c, cudaMemsetAsync(c->d_found, 0, sizeof(int), c->stream));
+    const unsigned long long blocks = std::min<unsigned long long>((count + 255) / 256, 148ull * 16);
+    dmin_sphere_kernel<<<(unsigned)blocks, 256, 0, c->stream>>>(n, (uint32_t)sb, (int)target, d, count,
+                                                                 c->d_binom, c->d_found);
+    BK_CUDA(c, cudaGetLastError());
+    int found = 0;
+    BK_CUDA(c, cudaMemcpyAsync(&found, c->d_found, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    BK_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (found) {
+      *d_out = d;
+      return BK_OK;
+    }
+  }
+  *d_out = not_found;
+  return BK_OK;
+}
+
+void bk_sampling_result_release(bk_sampling_result* r) {
+  if (!r) return;
+  free(r->unique_basis);
+  free(r->seed_stats);
+  free(r->time_points);
+  free(r->p_less_history);
+  free(r->dh_history);
+  std::memset(r, 0, sizeof(*r));
+}
+
+int bk_sampler_run(bk_ctx* c, const bk_sampler_config* cfg, uint64_t start_bits, bk_sampling_result* out) {
+  if (!c || !cfg || !out) return BK_ERR_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  const int n = cfg->n;
+  // reference: sampler.cuh:416-418 (n > 30 is out of the statevector backend's range)
+  if (n > 30) return fail(c, BK_ERR_UNSUPPORTED, "statevector backend supports n <= 30 (got %d)", n);
+  if (n < 1) return fail(c, BK_ERR_INVALID, "n = %d", n);
+  if (!(cfg->dt > 0.0) || !is_finite(cfg->dt) || !is_finite(cfg->t_max) || !is_finite(cfg->g) ||
+      !is_finite(cfg->t_start) || !is_finite(cfg->dt_sample) || !is_finite(cfg->dt_trajectory))
+    return fail(c, BK_ERR_INVALID, "non-finite or non-positive time parameters");
+  const uint64_t m = (1ull << n) - 1ull;
+  const int64_t E0 = host_energy(n, start_bits & m);
+  out->start_energy = E0;
+  int dmin = 0;
+  BK_TRY(bk_d_min(c, n, start_bits, E0, -1, &dmin));
+  out->d_min = dmin;
+  uint64_t below = 0;
+  BK_TRY(bk_p_blind(c, n, E0, &below, &out->p_blind));
+
+  // ---- schedule (sampler.cuh:496-602): measurement and sampling flags per step
+  const int T = (int)std::round(cfg->t_max / cfg->dt);
+  if (T < 0 || T > 100000000) return fail(c, BK_ERR_INVALID, "t_max / dt gives %d steps", T);
+  const double sample_interval = (cfg->dt_sample > 0.0) ? cfg->dt_sample
+                                                        : (cfg->t_max / std::max(1, cfg->num_sample_points));
+  double next_sample = cfg->t_start;
+  const double traj_interval = (cfg->dt_trajectory > 0.0) ? cfg->dt_trajectory : cfg->dt;
+  double next_traj = 0.0;
+  const double sample_end = (cfg->num_sample_points > 1 && cfg->dt_sample > 0.0)
+                                ? (cfg->t_start + (cfg->num_sample_points - 1) * cfg->dt_sample)
+                                : cfg->t_max;
+  int taken = 0;
+  std::vector<uint8_t> meas((size_t)T + 1, 0), samp((size_t)T + 1, 0);
+  std::vector<double> times;
+  std::vector<int> sample_steps;
+  for (int step = 0; step <= T; ++step) {
+    const double t = step * cfg->dt;
+    if (cfg->record_trajectory) {
+      if (t >= next_traj - 1e-9 && next_traj <= cfg->t_max + 1e-9) {
+        meas[(size_t)step] = 1;
+        times.push_back(t);
+        next_traj += traj_interval;
+      }
+    } else if (cfg->track_p_less) {
+      if (t >= next_sample - 1e-9 && next_sample <= cfg->t_max + 1e-9) {
+        meas[(size_t)step] = 1;
+        times.push_back(t);
+      }
+    }
+    if (cfg->shots_per_point > 0 && t >= cfg->t_start - 1e-9 && t >= next_sample - 1e-9 &&
+        next_sample <= sample_end + 1e-9 && (cfg->num_sample_points <= 0 || taken < cfg->num_sample_points)) {
+      ++taken;
+      samp[(size_t)step] = 1;
+      sample_steps.push_back(step);
+      next_sample += sample_interval;
+    } else if (cfg->shots_per_point == 0 && !cfg->record_trajectory && cfg->track_p_less &&
+               t >= next_sample - 1e-9 && next_sample <= cfg->t_max + 1e-9) {
+      next_sample += sample_interval;
+    }
+  }
+
+  // ---- random numbers in the reference's order (sampler.cuh:476-487, 567-568)
+  const int shots = std::max(1, cfg->shots_per_point);
+  const int n_seeds = std::max(1, cfg->num_sampling_seeds);
+  std::vector<std::mt19937_64> rngs((size_t)n_seeds);
+  for (int s = 0; s < n_seeds; ++s) rngs[(size_t)s].seed(cfg->seed + (uint64_t)s * cfg->seed_stride);
+  std::uniform_real_distribution<double> dist(0.0, 1.0);
+  const size_t per_point = (size_t)n_seeds * (size_t)shots;
+  std::vector<double> rnd(sample_steps.size() * per_point);
+  for (size_t pt = 0; pt < sample_steps.size(); ++pt)
+    for (int s = 0; s < n_seeds; ++s)
+      for (int i = 0; i < shots; ++i) rnd[pt * per_point + (size_t)s * shots + (size_t)i] = dist(rngs[(size_t)s]);
+  std::vector<uint64_t> drawn(rnd.size());
+
+  bk_evolve_params ep;
+  std::memset(&ep, 0, sizeof(ep));
+  ep.n = n;
+  ep.precision = cfg->precision;
+  ep.method = cfg->method;
+  ep.ordering = BK_ORDER_REFERENCE;
+  ep.s0 = start_bits & m;
+  ep.e0 = E0;
+  ep.dt = cfg->dt;
+  ep.diag_scale = 0.0;
+  ep.n_steps = T;
+  ep.g = nullptr;
+  ep.g_const = cfg->g;
+  ep.measure = meas.data();
+  if (!sample_steps.empty()) {
+    ep.sample = samp.data();
+    ep.shots = (int32_t)per_point;
+    ep.randnums = rnd.data();
+    ep.samples_out = drawn.data();
+  }
+  std::vector<double> pl(times.size()), dh(times.size());
+  BK_TRY(bk_evolve(c, &ep, pl.data(), dh.data(), nullptr));
+
+  // ---- per-shot statistics (sampler.cuh:575-597)
+  std::vector<bk_seed_stats> ss((size_t)n_seeds);
+  for (int s = 0; s < n_seeds; ++s) {
+    std::memset(&ss[(size_t)s], 0, sizeof(bk_seed_stats));
+    ss[(size_t)s].seed = cfg->seed + (uint64_t)s * cfg->seed_stride;
+    ss[(size_t)s].best_energy = E0;
+  }
+  std::unordered_set<uint64_t> uniq;
+  uint64_t flips_primary = 0;
+  for (size_t pt = 0; pt < sample_steps.size(); ++pt) {
+    for (int s = 0; s < n_seeds; ++s) {
+      uint64_t flips = 0;
+      for (int i = 0; i < shots; ++i) {
+        const uint64_t b = drawn[pt * per_point + (size_t)s * shots + (size_t)i];
+        uniq.insert(b);
+        const int d = __builtin_popcountll(start_bits ^ b);
+        flips += (uint64_t)d;
+        if (s == 0) flips_primary += (uint64_t)d;
+        const int64_t e = host_energy(n, b);
+        if (e < ss[(size_t)s].best_energy) ss[(size_t)s].best_energy = e;
+        if (e < E0) {
+          ss[(size_t)s].improved_shots++;
+          if (s == 0) out->improved_shots++;
+        }
+      }
+      ss[(size_t)s].total_shots_collected += (uint64_t)shots;
+      ss[(size_t)s].mean_hamming_flips += (double)flips;
+    }
+    out->total_shots_collected += (uint64_t)shots;
+  }
+
+  // ---- post-processing (sampler.cuh:621-683)
+  out->total_evals = out->total_shots_collected;
+  if (out->total_shots_collected > 0) {
+    out->mean_hamming_flips = (double)flips_primary / (double)out->total_shots_collected;
+    out->success_rate = (double)out->improved_shots / (double)out->total_shots_collected;
+    out->per_eval_rate = out->total_evals > 0 ? (double)out->improved_shots / (double)out->total_evals : 0.0;
+  }
+  for (auto& x : ss) {
+    if (x.total_shots_collected > 0) {
+      x.success_rate = (double)x.improved_shots / (double)x.total_shots_collected;
+      x.per_eval_rate = x.success_rate;
+      x.mean_hamming_flips /= (double)x.total_shots_collected;
+    }
+  }
+  const size_t np = times.size();
+  for (size_t i = 0; i < np; ++i)
+    if (pl[i] > out->peak_p_less) {
+      out->peak_p_less = pl[i];
+      out->peak_time = times[i];
+    }
+  if (np > 0) {
+    size_t first_drop = np - 1;
+    for (size_t i = 1; i < np; ++i)
+      if (pl[i] < pl[i - 1]) {
+        first_drop = i - 1;
+        break;
+      }
+    const double tp = times[first_drop];
+    out->initial_rise_rate_avg = (tp > 0.0) ? pl[first_drop] / tp : 0.0;
+    double mx = (times[0] > 1e-9) ? pl[0] / times[0] : 0.0;
+    for (size_t i = 0; i < first_drop; ++i) {
+      const double h = times[i + 1] - times[i];
+      if (h > 1e-9) mx = std::max(mx, (pl[i + 1] - pl[i]) / h);
+    }
+    out->initial_rise_rate_max = mx;
+  }
+  {
+    const double a0 = cfg->t_start;
+    const double a1 = (cfg->num_sample_points > 1 && cfg->dt_sample > 0.0)
+                          ? (cfg->t_start + (cfg->num_sample_points - 1) * cfg->dt_sample)
+                          : cfg->t_max;
+    double sum = 0.0;
+    size_t cnt = 0;
+    for (size_t i = 0; i < np; ++i)
+      if (times[i] >= a0 - 1e-9 && times[i] <= a1 + 1e-9) {
+        sum += dh[i];
+        ++cnt;
+      }
+    out->window_avg_dh = cnt > 0 ? sum / (double)cnt : (np > 0 ? dh[np - 1] : 0.0);
+  }
+
+  // ---- hand the arrays over (library-owned until bk_sampling_result_release)
+  std::vector<uint64_t> ub(uniq.begin(), uniq.end());
+  std::sort(ub.begin(), ub.end());
+  out->unique_basis_size = (int64_t)ub.size();
+  out->n_points = (int64_t)np;
+  out->n_seed_stats = n_seeds;
+  out->unique_basis = static_cast<uint64_t*>(malloc(std::max<size_t>(ub.size(), 1) * sizeof(uint64_t)));
+  out->seed_stats = static_cast<bk_seed_stats*>(malloc(ss.size() * sizeof(bk_seed_stats)));
+  out->time_points = static_cast<double*>(malloc(std::max<size_t>(np, 1) * sizeof(double)));
+  out->p_less_history = static_cast<double*>(malloc(std::max<size_t>(np, 1) * sizeof(double)));
+  out->dh_history = static_cast<double*>(malloc(std::max<size_t>(np, 1) * sizeof(double)));
+  if (!out->unique_basis || !out->seed_stats || !out->time_points || !out->p_less_history || !out->dh_history) {
+    bk_sampling_result_release(out);
+    return fail(c, BK_ERR_OOM, "host allocation of the sampling result failed");
+  }
+  std::copy(ub.begin(), ub.end(), out->unique_basis);
+  std::copy(ss.begin(), ss.end(), out->seed_stats);
+  std::copy(times.begin(), times.end(), out->time_points);
+  std::copy(pl.begin(), pl.end(), out->p_less_history);
+  std::copy(dh.begin(), dh.end(), out->dh_history);
+
+  if (cfg->verbose) {
+    // the reference's console report (sampler.cuh:529-539, 686-696), replayed from the recorded series
+    if (cfg->record_trajectory) {
+      double peak = 0.0, peak_t = 0.0;
+      for (size_t i = 0; i < np; ++i) {
+        if (pl[i] > peak) {
+          peak = pl[i];
+          peak_t = times[i];
+        }
+        const int step = (int)std::llround(times[i] / cfg->dt);
+        if (step % 200 == 0 || step == T) {
+          const double pct = (T > 0) ? (100.0 * step / T) : 100.0;
+          std::cout << "    [Progress " << std::setw(3) << (int)pct << "%] Step " << std::setw(4) << step << "/" << T
+                    << " (t = " << std::fixed << std::setprecision(1) << times[i] << "s)"
+                    << " | P_<(t) = " << std::scientific << std::setprecision(3) << pl[i]
+                    << " | <dH> = " << std::fixed << std::setprecision(2) << dh[i] << " | Peak = " << peak
+                    << " (at t=" << std::fixed << std::setprecision(1) << peak_t << "s)" << std::defaultfloat
+                    << std::endl;
+        }
+      }
+    }
+    std::cout << "[Quantum Sampler] Successes / Trials: " << out->improved_shots << " / "
+              << out->total_shots_collected << " (" << std::fixed << std::setprecision(2)
+              << (out->success_rate * 100.0) << "%)" << " | E < E_og (E_og = " << E0 << ")"
+              << " | Window <dH>: " << std::fixed << std::setprecision(2) << out->window_avg_dh
+              << " | Rise Rate (avg): " << std::scientific << std::setprecision(3) << out->initial_rise_rate_avg
+              << " | Evals: " << out->total_evals << " | Per-Eval Rate: " << std::scientific
+              << std::setprecision(4) << out->per_eval_rate << std::defaultfloat << "\n";
+  }
   return BK_OK;
 }
 

@@ -34,10 +34,8 @@ struct PassParams {
   int32_t hi_dim;     // TMA dim carrying the [h0 + W, n) coordinate (-1: none)
   R t;                // tan(g dt) of this step
   // A1 / measure-only
-  const typename AmpTraits<R>::amp* phase_hi;
-  const typename AmpTraits<R>::amp* phase_lo;
-  int32_t n_hi;
-  R amp_scale;        // exact power of two folded into D (overflow guard)
+  typename PhaseOf<R>::params phase;
+  R amp_scale;        // exact power of two applied with D (overflow guard); 1 = none
   int32_t measure;    // measure this step (A1) — measure-only kernels always do
   int32_t slot;       // results row
   int32_t e0;         // P_< threshold
@@ -176,8 +174,7 @@ template <class R>
 struct SmemLayout {
   static constexpr int kTileBytes = (1 << AmpTraits<R>::kTileBits) * (int)sizeof(typename AmpTraits<R>::amp);
   static constexpr int kEBytes = (1 << AmpTraits<R>::kTileBits) * 2;
-  static constexpr int kHiMax = 72;  // > (8555 >> 7) + 1 entries at n = 30
-  static constexpr int kTablesBytes = (kHiMax + kPhaseLo) * (int)sizeof(typename AmpTraits<R>::amp);
+  static constexpr int kTablesBytes = PhaseOf<R>::kSmemBytes;
   static constexpr int kA1Bytes = kTileBytes + kEBytes + kTablesBytes + 16;
   static constexpr int kStridedBytes = kTileBytes + 16;
 };
@@ -225,20 +222,11 @@ __global__ void __launch_bounds__(kThreads, 2)
   extern __shared__ __align__(1024) unsigned char smem[];
   amp* tile = reinterpret_cast<amp*>(smem);
   uint16_t* etile = reinterpret_cast<uint16_t*>(smem + L::kTileBytes);
-  amp* ph_hi = reinterpret_cast<amp*>(smem + L::kTileBytes + L::kEBytes);
-  amp* ph_lo = ph_hi + L::kHiMax;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::kTileBytes + L::kEBytes + L::kTablesBytes);
 
   // tables for D (overlaps the TMA)
-  if (KIND == 0) {
-    for (int i = threadIdx.x; i < p.n_hi; i += kThreads) {
-      amp h = p.phase_hi[i];
-      h.x *= p.amp_scale;
-      h.y *= p.amp_scale;
-      ph_hi[i] = h;
-    }
-    for (int i = threadIdx.x; i < kPhaseLo; i += kThreads) ph_lo[i] = p.phase_lo[i];
-  }
+  typename PhaseOf<R>::Smem tabs{};
+  if (KIND == 0) tabs = PhaseOf<R>::stage(p.phase, smem + L::kTileBytes + L::kEBytes);
   if (!load_tile<R>(&amap, &emap, tile, etile, bar, -1, 0, p.hi_dim, (int)blockIdx.x, p.err,
                     (uint32_t)(L::kTileBytes + L::kEBytes)))
     return;
@@ -257,7 +245,14 @@ __global__ void __launch_bounds__(kThreads, 2)
     const uint32_t i = b1 | pdep((uint32_t)j, PL::A1_R1_REG);
     const int e = (int)etile[i];
     if (do_measure) acc.add(norm2d(v[j]), e < p.e0, __popc((tile_base | i) ^ p.s0));
-    if (KIND == 0) v[j] = cmul(v[j], cmul(ph_hi[e >> kPhaseLoBits], ph_lo[e & (kPhaseLo - 1)]));
+    if (KIND == 0) v[j] = PhaseOf<R>::apply(v[j], e, p.phase, tabs);
+  }
+  if (KIND == 0 && p.amp_scale != (R)1) {
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+      v[j].x *= p.amp_scale;
+      v[j].y *= p.amp_scale;
+    }
   }
   if (KIND == 0) {
     butterflies<R, PL::A1_R1_REG, PL::A1_R1_REG>(v, p.t);

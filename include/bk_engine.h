@@ -100,6 +100,15 @@ typedef struct bk_evolve_params {
   double g_const;      /* field used when g == NULL */
   const uint8_t* measure; /* host, n_steps + 1 flags: measure BEFORE step k (k = n_steps: final) */
   double norm_tol;     /* > 0: fail with BK_ERR_NORM when | |psi|^2 - 1 | > norm_tol at a measured step */
+  /* projective sampling inside the run (sampler.cuh:559-598): at every flagged
+   * step k, `shots` basis states are drawn from |psi_k|^2 (inverse CDF, FP64
+   * prefix sums) using the next `shots` host uniforms; results in random-number
+   * order. sample == NULL disables sampling. */
+  const uint8_t* sample;    /* host, n_steps + 1 flags */
+  int32_t shots;            /* draws per flagged step */
+  int32_t reserved1;
+  const double* randnums;   /* host, (#flagged) * shots uniforms in [0, 1) */
+  uint64_t* samples_out;    /* host, (#flagged) * shots basis states */
 } bk_evolve_params;
 
 /* Runs the whole schedule on the device and returns one row per flagged step:
@@ -118,6 +127,77 @@ int bk_kernel_timing(bk_ctx* ctx, int index, const char** name, int64_t* launche
 /* The context's CUDA stream (a cudaStream_t) so callers can order their own
  * work and record CUDA events around the engine's launches. */
 int bk_stream(bk_ctx* ctx, void** stream_out);
+
+/* ---- The reference's ISampler::sample() (sampler.cuh:303-310, 412-707) ---- */
+
+/* SamplerConfig (sampler.cuh:235-260) plus the engine's precision / method. */
+typedef struct bk_sampler_config {
+  int32_t n;
+  int32_t num_sample_points;
+  int32_t shots_per_point;
+  int32_t num_sampling_seeds;
+  int32_t track_p_less;
+  int32_t record_trajectory;
+  int32_t verbose;
+  int32_t precision;        /* bk_precision (the reference computes in complex128) */
+  int32_t method;           /* bk_method */
+  int32_t reserved;
+  uint64_t seed;
+  uint64_t seed_stride;
+  double g, dt, t_max, t_start, dt_sample, dt_trajectory;
+} bk_sampler_config;
+
+/* SeedSamplingStats (sampler.cuh:262-270). */
+typedef struct bk_seed_stats {
+  uint64_t seed;
+  uint64_t total_shots_collected;
+  uint64_t improved_shots;
+  double success_rate;
+  double per_eval_rate;
+  double mean_hamming_flips;
+  int64_t best_energy;
+} bk_seed_stats;
+
+/* SamplingResult (sampler.cuh:272-297). Arrays are allocated by the library and
+ * freed by bk_sampling_result_release. */
+typedef struct bk_sampling_result {
+  uint64_t* unique_basis;
+  int64_t unique_basis_size;
+  uint64_t total_shots_collected;
+  uint64_t improved_shots;
+  double success_rate;
+  double per_eval_rate;
+  uint64_t total_evals;
+  double mean_hamming_flips;
+  bk_seed_stats* seed_stats;
+  int32_t n_seed_stats;
+  int32_t d_min;
+  double* time_points;
+  double* p_less_history;
+  double* dh_history;
+  int64_t n_points;
+  double window_avg_dh;
+  double initial_rise_rate_avg;
+  double initial_rise_rate_max;
+  int64_t start_energy;
+  double p_blind;
+  double peak_p_less;
+  double peak_time;
+} bk_sampling_result;
+
+/* Full sample() semantics: E0 and d_min of the start state, p_blind, the
+ * measurement / sampling schedule with the reference's time accumulators and
+ * 1e-9 tolerances, shots drawn with mt19937_64(seed + s * seed_stride) and
+ * uniform_real_distribution<double>(0, 1) in the reference's order, per-shot
+ * statistics and the post-processing of rise rates and window averages.
+ * n > 30 returns BK_ERR_UNSUPPORTED (the reference throws). */
+int bk_sampler_run(bk_ctx* ctx, const bk_sampler_config* cfg, uint64_t start_bits, bk_sampling_result* out);
+void bk_sampling_result_release(bk_sampling_result* r);
+
+/* d_min: smallest Hamming distance from s to a state with E < target (target < 0:
+ * E(s)); n (or max_d + 1) when none exists or target <= E*(n)
+ * (labs_energy.hpp:175-207). Hamming spheres are enumerated on the device. */
+int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* d_out);
 
 /* ---- Projective sampling (sampler.cuh:459-487, 559-598) ---- */
 
