@@ -332,7 +332,7 @@ int build_phase(bk_ctx* c, int n, double angle_unit, Phase32* P) {
   for (;; n_h *= 2) {
     if (n_h > kPhaseH)
       return fail(c, BK_ERR_UNSUPPORTED, "phase angle per unit energy %g too large for the table", angle_unit);
-    K = (uint32_t)((emax + n_h) / n_h);  // ceil((emax + 1) / n_h)
+    K = std::max<uint32_t>(2u, (uint32_t)((emax + n_h) / n_h));  // ceil((emax + 1) / n_h), >= 2 so M fits 32 bits
     if (std::fabs(angle_unit) * (double)(K - 1) <= 0.5) break;
   }
   const uint32_t M = (uint32_t)((((uint64_t)1 << 32) + K - 1) / K);
