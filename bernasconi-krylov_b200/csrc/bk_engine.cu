@@ -767,6 +767,7 @@ const char* bk_status_string(int s) {
     case BK_ERR_NORM: return "norm outside tolerance";
     case BK_ERR_UNSUPPORTED: return "unsupported configuration";
     case BK_ERR_NO_DEVICE: return "no usable CUDA device";
+    case BK_ERR_TOO_LARGE: return "request beyond a fixed limit (bk_measure_noalloc: n <= 30)";
     default: return "unknown status";
   }
 }

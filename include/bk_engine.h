@@ -26,7 +26,8 @@ typedef enum bk_status {
   BK_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up (kernel returned early) */
   BK_ERR_NORM = 5,        /* |psi|^2 left the tolerance band at a measured step */
   BK_ERR_UNSUPPORTED = 6, /* configuration not provided by this build (e.g. n > 30) */
-  BK_ERR_NO_DEVICE = 7    /* no CUDA device / not an sm_100 device */
+  BK_ERR_NO_DEVICE = 7,   /* no CUDA device / not an sm_100 device */
+  BK_ERR_TOO_LARGE = 8    /* request beyond a fixed limit (bk_measure_noalloc: n <= 30) */
 } bk_status;
 
 typedef enum bk_precision { BK_C64 = 0, BK_C128 = 1 } bk_precision;
@@ -204,6 +205,28 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
 /* Samples `shots` basis states from |psi|^2 of the state left by the last
  * bk_evolve: inverse CDF (FP64 prefix sums), results in random-number order. */
 int bk_sample(bk_ctx* ctx, const double* randnums, int64_t shots, uint64_t* out_states);
+
+/* ---- Measurement without device allocation ----
+ *
+ * No counterpart in the reference. For callers that cannot let a library
+ * allocate device memory — a host framework that owns all GPU memory through
+ * its own allocator or fixed arena, or a latency-critical loop that must not
+ * synchronise on an allocation: measures a caller-owned statevector and writes
+ * d_out[0] = P_< (sum of |psi_s|^2 over E(s) < e0; e0 < 0 means E(s0)),
+ * d_out[1] = <d_H> (weights popcount(s ^ s0)), d_out[2] = |psi|^2, all FP64.
+ *   d_state: device, 2^n amplitudes, interleaved (re, im), float (BK_C64) or
+ *            double (BK_C128), natural index order; d_out: device, 3 doubles;
+ *   stream:  a cudaStream_t (NULL = the legacy default stream); the call only
+ *            enqueues work (read d_out after synchronising that stream).
+ * Allocates nothing: its scratch is a fixed 24.25 KiB array inside the library
+ * (1024 block partial sums and a ticket), which every GPU that loads the
+ * library holds until the process exits. Limit: 1 <= n <= 30, else
+ * BK_ERR_TOO_LARGE. The first call on a device resolves the array's device
+ * address; make that first call before any stream capture. All calls share the
+ * array (it keeps the last call's contents; the ticket is cleared at the start
+ * of every call), so calls that overlap on the GPU race: serialise them. */
+int bk_measure_noalloc(int n, int precision, const void* d_state, int64_t e0, uint64_t s0, double* d_out,
+                       void* stream);
 
 #ifdef __cplusplus
 }
