@@ -46,6 +46,24 @@ __global__ void set_basis_kernel(A* psi, uint32_t idx) {
   psi[idx] = one;
 }
 
+// complex64 pair-planar storage: float4 k = (re[2k], re[2k+1], im[2k], im[2k+1])
+struct Planar64 {};
+__global__ void set_basis_planar_kernel(float* psi, uint32_t idx) { psi[4u * (idx >> 1) + (idx & 1u)] = 1.0f; }
+__device__ __forceinline__ double norm2_at(const float2* psi, uint32_t i) { return norm2d(psi[i]); }
+__device__ __forceinline__ double norm2_at(const double2* psi, uint32_t i) { return norm2d(psi[i]); }
+__device__ __forceinline__ double norm2_at(const Planar64* psi, uint32_t i) {
+  const float* f = reinterpret_cast<const float*>(psi) + 4u * (i >> 1) + (i & 1u);
+  return (double)fmaf(f[0], f[0], f[2] * f[2]);
+}
+__device__ __forceinline__ double2 amp_at(const float2* psi, uint32_t i) {
+  return make_double2(psi[i].x, psi[i].y);
+}
+__device__ __forceinline__ double2 amp_at(const double2* psi, uint32_t i) { return psi[i]; }
+__device__ __forceinline__ double2 amp_at(const Planar64* psi, uint32_t i) {
+  const float* f = reinterpret_cast<const float*>(psi) + 4u * (i >> 1) + (i & 1u);
+  return make_double2(f[0], f[2]);
+}
+
 // ---------------------------------------------------------------------------
 // Whole-state kernel (n <= T): one CTA keeps the 2^n amplitudes in shared
 // memory and runs every step (measure if flagged, D, Rx on each qubit) in one
@@ -201,8 +219,8 @@ __global__ void export_kernel(const A* __restrict__ psi, const uint16_t* __restr
                               double angle_unit, double scale, double2* __restrict__ out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
-  const A a = psi[i];
-  double2 r = make_double2((double)a.x * scale, (double)a.y * scale);
+  const double2 a = amp_at(psi, i);
+  double2 r = make_double2(a.x * scale, a.y * scale);
   if (angle_unit != 0.0) {
     double sn, cs;
     sincos(-angle_unit * (double)E[i], &sn, &cs);
@@ -226,7 +244,7 @@ __global__ void chunk_sums_kernel(const A* __restrict__ psi, uint32_t count, dou
   const uint32_t base = chunk << kSampleChunkBits;
   const uint32_t len = min(1u << kSampleChunkBits, count - base);
   double acc = 0.0;
-  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) acc += norm2d(psi[base + i]);
+  for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) acc += norm2_at(psi, base + i);
   __shared__ double red[kThreads / 32];
   acc = warp_sum(acc);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
@@ -296,7 +314,7 @@ __global__ void sample_kernel(const A* __restrict__ psi, uint32_t count, const d
   const uint32_t per = (len + 31) / 32;
   const uint32_t mine0 = min(len, lane * per), mine1 = min(len, mine0 + per);
   double part = 0.0;
-  for (uint32_t i = mine0; i < mine1; ++i) part += norm2d(psi[base + i]);
+  for (uint32_t i = mine0; i < mine1; ++i) part += norm2_at(psi, base + i);
   double inc = part;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -314,7 +332,7 @@ __global__ void sample_kernel(const A* __restrict__ psi, uint32_t count, const d
       double c = start;
       uint32_t r = mine1 - 1;
       for (uint32_t i = mine0; i < mine1; ++i) {
-        c += norm2d(psi[base + i]);
+        c += norm2_at(psi, base + i);
         if (target < c) {
           r = i;
           break;

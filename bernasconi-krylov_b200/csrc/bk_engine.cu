@@ -22,6 +22,7 @@
 #include "bk_aux.cuh"
 #include "bk_engine.h"
 #include "bk_fused.cuh"
+#include "bk_persist.cuh"
 
 using namespace bk;
 
@@ -81,10 +82,15 @@ struct bk_ctx {
   size_t samples_cap = 0;
   unsigned long long* d_binom = nullptr;
   int* d_found = nullptr;
+  void* d_persist = nullptr;  // persistent engine: maps, descriptors, tasks, per-step arrays, counters
+  size_t persist_cap = 0;
+  int num_sms = 148;
+  bool planar = false;        // complex64 state stored pair-planar (persistent engine)
   // tensor maps, keyed by (state ptr, n, precision, pass)
   std::map<std::string, TmaDesc> tma;
   // last evolution (for export / sampling)
   bool have_state = false;
+  bool last_planar = false;
   int last_n = 0, last_prec = 0, last_ordering = 0;
   long double last_log2_scale = 0.0L;
   double last_angle_unit = 0.0;
@@ -399,7 +405,7 @@ struct Schedule {
 // Projective sampling of the current state at sampling point `pt`: chunk sums
 // of |psi|^2, exclusive scan, one warp per draw.
 template <class A>
-int launch_sampling(bk_ctx* c, const A* psi, int n, int pt, int shots) {
+int launch_sampling_t(bk_ctx* c, const A* psi, int n, int pt, int shots) {
   const uint32_t count = 1u << n;
   const uint32_t m = (count + (1u << kSampleChunkBits) - 1) >> kSampleChunkBits;
   BK_TRY(ensure_buffer(c, reinterpret_cast<void**>(&c->d_chunks), &c->chunks_cap, (m + 1) * sizeof(double)));
@@ -412,6 +418,11 @@ int launch_sampling(bk_ctx* c, const A* psi, int n, int pt, int shots) {
                                                   shots, c->d_samples + (size_t)pt * shots);
   BK_CUDA(c, cudaGetLastError());
   return ev_end(c, ev);
+}
+template <class A>
+int launch_sampling(bk_ctx* c, const A* psi, int n, int pt, int shots) {
+  if (c->planar) return launch_sampling_t(c, reinterpret_cast<const Planar64*>(psi), n, pt, shots);
+  return launch_sampling_t(c, psi, n, pt, shots);
 }
 
 template <class R>
@@ -462,6 +473,241 @@ int launch_strided(bk_ctx* c, int w, const PassParams<R>& pp, const TmaDesc* am,
     case 9: return launch_strided_w<R, 9>(c, pp, am, n);
     default: return fail(c, BK_ERR_UNSUPPORTED, "strided pass width %d", w);
   }
+}
+
+// ---------------------------------------------------------------------------
+// persistent dataflow engine (csrc/bk_persist.cuh)
+// ---------------------------------------------------------------------------
+// complex64 level table for the vectorised phase: hab[h] = {-tan(th/4), sin(th/2)}
+// for th = -angle_unit h K reduced to (-pi, pi], applied twice.
+int build_phase_v(bk_ctx* c, int n, double angle_unit, PhaseV32* P, std::vector<float2>* hab) {
+  const int emax = (n - 1) * n * (2 * n - 1) / 6;
+  int n_h = 16;
+  uint32_t K = 0;
+  for (;; n_h *= 2) {
+    if (n_h > kPhaseH)
+      return fail(c, BK_ERR_UNSUPPORTED, "phase angle per unit energy %g too large for the table", angle_unit);
+    K = std::max<uint32_t>(2u, (uint32_t)((emax + n_h) / n_h));
+    if (std::fabs(angle_unit) * (double)(K - 1) <= 0.5) break;
+  }
+  const uint32_t M = (uint32_t)((((uint64_t)1 << 32) + K - 1) / K);
+  for (uint64_t e = 0; e <= (uint64_t)emax; ++e)
+    if (((e * M) >> 32) != e / K) return fail(c, BK_ERR_UNSUPPORTED, "no exact level split for n = %d", n);
+  hab->resize((size_t)n_h);
+  const double two_pi = 6.283185307179586;
+  for (int h = 0; h < n_h; ++h) {
+    double th = std::remainder(-angle_unit * (double)h * (double)K, two_pi);  // [-pi, pi]
+    (*hab)[(size_t)h] = make_float2((float)(-std::tan(0.25 * th)), (float)std::sin(0.5 * th));
+  }
+  P->K = K;
+  P->M = M;
+  P->theta = (float)(-angle_unit);
+  P->theta_lo = (float)(-angle_unit - (double)P->theta);
+  P->n_h = n_h;
+  return BK_OK;
+}
+
+// bump allocator over the context's persistent-engine buffer (256-byte aligned pieces)
+struct Bump {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return o;
+  }
+};
+
+template <class R>
+int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double angle_unit,
+                   const std::vector<R>& tans, const std::vector<R>& scales) {
+  const int n = p->n;
+  const bool c64 = sizeof(R) == 4;
+  const int np = c64 ? n - 1 : n;  // element bits
+  const int rest = np - kElemBits;
+  if (rest < 1) return fail(c, BK_ERR_UNSUPPORTED, "persistent engine needs n > %d", kElemBits + (c64 ? 1 : 0));
+  const int w2 = (rest <= 9) ? rest : (rest + 1) / 2;
+  const int w3 = rest - w2;
+  if (w2 > 9 || w3 > 9) return fail(c, BK_ERR_UNSUPPORTED, "n = %d needs more than two strided passes", n);
+  const int e_tile_bits = c64 ? 13 : 12;
+
+  // tensor maps in element space (16-byte elements = two 8-byte TMA elements)
+  TmaDesc a1m, em, m2, m3;
+  BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits, kElemBits, 0, &a1m));
+  BK_TRY(build_e_map(c, c->d_E, n, e_tile_bits, &em));
+  BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w2, kElemBits, w2, &m2));
+  if (w3 > 0) BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w3, kElemBits + w2, w3, &m3));
+
+  // phase
+  typename PhaseV<R>::params ph{};
+  std::vector<float2> hab;
+  std::vector<double2> t64;
+  if constexpr (sizeof(R) == 4) {
+    BK_TRY(build_phase_v(c, n, angle_unit, &ph, &hab));
+  } else {
+    Phase64 p64{};
+    BK_TRY(build_phase(c, n, angle_unit, &p64));  // uploads to d_phase
+    ph.hi = p64.hi;
+    ph.lo = p64.lo;
+    ph.n_hi = p64.n_hi;
+  }
+
+  // tasks of one step: A1 of slab h+1 is queued ahead of S2 of slab h (L2 hand-off)
+  const uint32_t n_a1 = 1u << (np - kElemBits), n_s2 = n_a1, n_s3 = w3 > 0 ? n_a1 : 0u;
+  const uint32_t slabs = 1u << (np - kElemBits - w2);
+  const uint32_t per_slab = 1u << w2;
+  std::vector<unsigned long long> tasks;
+  tasks.reserve(n_a1 + n_s2 + n_s3);
+  auto task = [](int kind, int inst, uint32_t tile) {
+    return ((unsigned long long)kind << 56) | ((unsigned long long)inst << 32) | tile;
+  };
+  for (uint32_t h = 0; h <= slabs; ++h) {
+    if (h < slabs)
+      for (uint32_t j = 0; j < per_slab; ++j) tasks.push_back(task(TASK_A1, 0, h * per_slab + j));
+    if (h > 0)
+      for (uint32_t j = 0; j < per_slab; ++j) tasks.push_back(task(TASK_S2, 0, (h - 1) * per_slab + j));
+  }
+  for (uint32_t j = 0; j < n_s3; ++j) tasks.push_back(task(TASK_S3, 0, j));
+  std::vector<unsigned long long> final_tasks;
+  if (S.slot[(size_t)p->n_steps] >= 0)
+    for (uint32_t j = 0; j < n_a1; ++j) final_tasks.push_back(task(TASK_M, 0, j));
+
+  // device buffer layout
+  Bump b;
+  const size_t o_maps = b.take(4 * sizeof(CUtensorMap));
+  const size_t o_desc = b.take(sizeof(InstDesc<R>));
+  const size_t o_tasks = b.take(tasks.size() * 8);
+  const size_t o_final = b.take(std::max<size_t>(final_tasks.size(), 1) * 8);
+  const size_t o_tan = b.take(std::max<size_t>(tans.size(), 1) * sizeof(R));
+  const size_t o_scale = b.take(std::max<size_t>(scales.size(), 1) * sizeof(R));
+  const size_t o_slot = b.take(S.slot.size() * sizeof(int));
+  const size_t o_hab = b.take(std::max<size_t>(hab.size(), 1) * sizeof(float2));
+  const size_t o_ctr = b.take((slabs + 8) * sizeof(unsigned int));
+  const size_t o_part = b.take(3 * (size_t)n_a1 * sizeof(double));
+  BK_TRY(ensure_buffer(c, &c->d_persist, &c->persist_cap, b.off));
+  char* base = static_cast<char*>(c->d_persist);
+  CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(base + o_maps);
+  unsigned int* ctr = reinterpret_cast<unsigned int*>(base + o_ctr);
+  // counter block: [a1_done: slabs][s2_done][s3_done][ticket][next][err][abort]
+  unsigned int* a1_done = ctr;
+  unsigned int* s2_done = ctr + slabs;
+  unsigned int* s3_done = ctr + slabs + 1;
+  unsigned int* ticket = ctr + slabs + 2;
+  unsigned int* next = ctr + slabs + 3;
+  int* err = reinterpret_cast<int*>(ctr + slabs + 4);
+  int* abort_w = reinterpret_cast<int*>(ctr + slabs + 5);
+
+  CUtensorMap maps[4] = {a1m.map, em.map, m2.map, w3 > 0 ? m3.map : m2.map};
+  InstDesc<R> D{};
+  D.state = static_cast<unsigned char*>(c->d_state);
+  D.map_a1 = d_maps + 0;
+  D.map_e = d_maps + 1;
+  D.map_s2 = d_maps + 2;
+  D.map_s3 = d_maps + 3;
+  D.np = np;
+  D.n = n;
+  D.w2 = w2;
+  D.w3 = w3;
+  D.a1_hi_dim = a1m.hi_dim;
+  D.s2_mid_dim = m2.mid_dim;
+  D.s2_hi_dim = m2.hi_dim;
+  D.s2_mid_bits = (int)m2.mid_bits;
+  D.s3_mid_dim = w3 > 0 ? m3.mid_dim : -1;
+  D.s3_hi_dim = w3 > 0 ? m3.hi_dim : -1;
+  D.s3_mid_bits = w3 > 0 ? (int)m3.mid_bits : 0;
+  D.e0 = (int)p->e0;
+  D.s0 = (uint32_t)(p->s0 & ((1ull << n) - 1ull));
+  if constexpr (sizeof(R) == 4) ph.hab = reinterpret_cast<const float2*>(base + o_hab);
+  D.phase = ph;
+  D.tan = reinterpret_cast<const R*>(base + o_tan);
+  D.scale = reinterpret_cast<const R*>(base + o_scale);
+  D.slot = reinterpret_cast<const int*>(base + o_slot);
+  D.a1_done = a1_done;
+  D.s2_done = s2_done;
+  D.s3_done = s3_done;
+  D.ticket = ticket;
+  D.partials = reinterpret_cast<double*>(base + o_part);
+  D.results = c->d_results;
+  D.n_a1 = n_a1;
+  D.n_s2 = n_s2;
+  D.n_s3 = n_s3;
+  D.inverse = 0;
+
+  cudaStream_t st = c->stream;
+  BK_CUDA(c, cudaMemcpyAsync(d_maps, maps, sizeof(maps), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemcpyAsync(base + o_tasks, tasks.data(), tasks.size() * 8, cudaMemcpyHostToDevice, st));
+  if (!final_tasks.empty())
+    BK_CUDA(c, cudaMemcpyAsync(base + o_final, final_tasks.data(), final_tasks.size() * 8, cudaMemcpyHostToDevice, st));
+  if (!tans.empty()) {
+    BK_CUDA(c, cudaMemcpyAsync(base + o_tan, tans.data(), tans.size() * sizeof(R), cudaMemcpyHostToDevice, st));
+    BK_CUDA(c, cudaMemcpyAsync(base + o_scale, scales.data(), scales.size() * sizeof(R), cudaMemcpyHostToDevice, st));
+  }
+  BK_CUDA(c, cudaMemcpyAsync(base + o_slot, S.slot.data(), S.slot.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (!hab.empty())
+    BK_CUDA(c, cudaMemcpyAsync(base + o_hab, hab.data(), hab.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R>), PersistSmem::kBytes));
+
+  // one launch per segment between sampling points (sampling reads psi_k before step k)
+  using Samp = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
+  int k0 = 0, search = 0;
+  for (;;) {
+    int k1 = search;
+    while (k1 < p->n_steps && S.sample_pt[(size_t)k1] < 0) ++k1;
+    // launch steps [k0, k1) (+ the final measurement when k1 == n_steps)
+    D.tan = reinterpret_cast<const R*>(base + o_tan) + k0;
+    D.scale = reinterpret_cast<const R*>(base + o_scale) + k0;
+    D.slot = reinterpret_cast<const int*>(base + o_slot) + k0;
+    BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &D, sizeof(D), cudaMemcpyHostToDevice, st));
+    BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
+    Program P{};
+    P.tasks = reinterpret_cast<const unsigned long long*>(base + o_tasks);
+    P.per_step = (uint32_t)tasks.size();
+    P.n_steps = (uint32_t)(k1 - k0);
+    const bool last = (k1 == p->n_steps);
+    const bool sample_final = last && S.sample_pt[(size_t)k1] >= 0;
+    P.final_tasks = reinterpret_cast<const unsigned long long*>(base + o_final);
+    P.n_final = (last && !sample_final) ? (uint32_t)final_tasks.size() : 0u;
+    P.step0 = (uint32_t)k0;
+    P.next = next;
+    P.err = err;
+    P.abort = abort_w;
+    if (P.n_steps > 0 || P.n_final > 0) {
+      size_t ev = 0;
+      BK_TRY(ev_begin(c, "persist", &ev));
+      persist_kernel<R><<<c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
+          reinterpret_cast<const InstDesc<R>*>(base + o_desc), P);
+      BK_CUDA(c, cudaGetLastError());
+      BK_TRY(ev_end(c, ev));
+      int e = 0;
+      BK_CUDA(c, cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+      BK_CUDA(c, cudaStreamSynchronize(st));
+      if (e != 0) return fail(c, BK_ERR_TIMEOUT, "persistent engine: a bounded device wait gave up (%d)", e);
+    }
+    if (k1 >= p->n_steps && !sample_final) break;
+    // sampling point k1 (state psi_k1 is in place)
+    BK_TRY(launch_sampling_t(c, reinterpret_cast<const Samp*>(c->d_state), n, S.sample_pt[(size_t)k1], S.shots));
+    if (sample_final) {
+      // final measurement after sampling
+      if (!final_tasks.empty()) {
+        D.slot = reinterpret_cast<const int*>(base + o_slot) + k1;
+        BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &D, sizeof(D), cudaMemcpyHostToDevice, st));
+        BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
+        P.n_steps = 0;
+        P.n_final = (uint32_t)final_tasks.size();
+        size_t ev = 0;
+        BK_TRY(ev_begin(c, "persist", &ev));
+        persist_kernel<R><<<c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
+            reinterpret_cast<const InstDesc<R>*>(base + o_desc), P);
+        BK_CUDA(c, cudaGetLastError());
+        BK_TRY(ev_end(c, ev));
+        BK_CUDA(c, cudaStreamSynchronize(st));
+      }
+      break;
+    }
+    k0 = k1;
+    search = k1 + 1;
+    // the next segment starts at k1; its first A1 measures step k1 if flagged
+  }
+  return BK_OK;
 }
 
 // Fused / whole-state evolution in precision R. Fills results rows on device
@@ -567,69 +813,7 @@ int evolve_fused(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
     return BK_OK;
   }
 
-  // tiled passes
-  const int rest = n - T;
-  const int w2 = (rest <= 9) ? rest : (rest + 1) / 2;
-  const int w3 = rest - w2;
-  if (w2 > 9 || w3 > 9) return fail(c, BK_ERR_UNSUPPORTED, "n = %d needs more than two strided passes", n);
-  const TmaDesc *a1m = nullptr, *em = nullptr, *m2 = nullptr, *m3 = nullptr;
-  BK_TRY(get_map(c, "A1", n, p->precision, T, T, 0, &a1m));
-  BK_TRY(get_map(c, "E", n, p->precision, 0, 0, 0, &em));
-  BK_TRY(get_map(c, "S", n, p->precision, T - w2, T, w2, &m2));
-  if (w3 > 0) BK_TRY(get_map(c, "S", n, p->precision, T - w3, T + w2, w3, &m3));
-
-  PassParams<R> base{};
-  base.state = reinterpret_cast<amp*>(c->d_state);
-  base.n = (uint32_t)n;
-  base.phase = phase;
-  base.e0 = e0;
-  base.s0 = s0;
-  base.partials = c->d_partials;
-  base.ticket = c->d_ticket;
-  base.results = c->d_results;
-  base.err = c->d_err;
-  base.hi_dim = a1m->hi_dim;
-  base.mid_dim = -1;
-
-  for (int k = 0; k <= p->n_steps; ++k) {
-    const int slot = S.slot[(size_t)k];
-    if (S.sample_pt[(size_t)k] >= 0)
-      BK_TRY(launch_sampling<amp>(c, base.state, n, S.sample_pt[(size_t)k], S.shots));
-    if (k == p->n_steps) {
-      if (slot >= 0) {
-        PassParams<R> pp = base;
-        pp.slot = slot;
-        pp.measure = 1;
-        BK_TRY(launch_a1<R>(c, 1, pp, a1m, em, n));
-      }
-      break;
-    }
-    PassParams<R> pp = base;
-    pp.t = tans[(size_t)k];
-    pp.amp_scale = scales[(size_t)k];
-    pp.measure = slot >= 0 ? 1 : 0;
-    pp.slot = slot >= 0 ? slot : 0;
-    BK_TRY(launch_a1<R>(c, 0, pp, a1m, em, n));
-    PassParams<R> q2 = base;
-    q2.t = tans[(size_t)k];
-    q2.cprime = (uint32_t)(T - w2);
-    q2.h0 = (uint32_t)T;
-    q2.mid_bits = m2->mid_bits;
-    q2.mid_dim = m2->mid_dim;
-    q2.hi_dim = m2->hi_dim;
-    BK_TRY(launch_strided<R>(c, w2, q2, m2, n));
-    if (w3 > 0) {
-      PassParams<R> q3 = base;
-      q3.t = tans[(size_t)k];
-      q3.cprime = (uint32_t)(T - w3);
-      q3.h0 = (uint32_t)(T + w2);
-      q3.mid_bits = m3->mid_bits;
-      q3.mid_dim = m3->mid_dim;
-      q3.hi_dim = m3->hi_dim;
-      BK_TRY(launch_strided<R>(c, w3, q3, m3, n));
-    }
-  }
-  return BK_OK;
+  return evolve_persist<R>(c, p, S, angle_unit, tans, scales);
 }
 
 // Plain path (reference launch structure), exact gates: no scale tracking.
@@ -786,6 +970,7 @@ int bk_create(int device, bk_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess) return BK_ERR_CUDA;
   bk_ctx* c = new bk_ctx();
   c->device = device;
+  c->num_sms = prop.multiProcessorCount;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&c->d_ticket, sizeof(unsigned int)) != cudaSuccess ||
       cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess ||
@@ -974,7 +1159,10 @@ int bk_evolve(bk_ctx* c, const bk_evolve_params* p, double* p_less, double* d_h,
   BK_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
   BK_CUDA(c, cudaMemsetAsync(c->d_state, 0, (1ull << n) * amp_bytes(p->precision), c->stream));
   const uint32_t s0 = (uint32_t)(p->s0 & ((1ull << n) - 1ull));
-  if (p->precision == BK_C64)
+  c->planar = (p->precision == BK_C64 && p->method == BK_FUSED && n > 13);
+  if (c->planar)
+    set_basis_planar_kernel<<<1, 1, 0, c->stream>>>(reinterpret_cast<float*>(c->d_state), s0);
+  else if (p->precision == BK_C64)
     set_basis_kernel<float2><<<1, 1, 0, c->stream>>>(reinterpret_cast<float2*>(c->d_state), s0);
   else
     set_basis_kernel<double2><<<1, 1, 0, c->stream>>>(reinterpret_cast<double2*>(c->d_state), s0);
@@ -1004,6 +1192,7 @@ int bk_evolve(bk_ctx* c, const bk_evolve_params* p, double* p_less, double* d_h,
   BK_TRY(check_device_error(c));
   BK_TRY(collect_timing(c));
   c->have_state = true;
+  c->last_planar = c->planar;
   c->last_n = n;
   c->last_prec = p->precision;
   c->last_ordering = p->ordering;
@@ -1321,7 +1510,10 @@ int bk_export_state(bk_ctx* c, double* host) {
   const double scale = (double)std::exp2(-c->last_log2_scale);
   const double ang = (c->last_ordering == BK_ORDER_STRANG) ? 0.5 * c->last_angle_unit : 0.0;
   const unsigned th = 256;
-  if (c->last_prec == BK_C64)
+  if (c->last_planar)
+    export_kernel<Planar64><<<(count + th - 1) / th, th, 0, c->stream>>>(
+        reinterpret_cast<const Planar64*>(c->d_state), c->d_E, count, ang, scale, reinterpret_cast<double2*>(c->d_io));
+  else if (c->last_prec == BK_C64)
     export_kernel<float2><<<(count + th - 1) / th, th, 0, c->stream>>>(
         reinterpret_cast<const float2*>(c->d_state), c->d_E, count, ang, scale, reinterpret_cast<double2*>(c->d_io));
   else
@@ -1348,7 +1540,12 @@ int bk_sample(bk_ctx* c, const double* randnums, int64_t shots, uint64_t* out) {
   BK_CUDA(c, cudaMemcpyAsync(d_rand, randnums, (size_t)shots * 8, cudaMemcpyHostToDevice, c->stream));
   const unsigned th = 256;
   const unsigned sblocks = (unsigned)(((size_t)shots * 32 + th - 1) / th);
-  if (c->last_prec == BK_C64) {
+  if (c->last_planar) {
+    auto psi = reinterpret_cast<const Planar64*>(c->d_state);
+    chunk_sums_kernel<Planar64><<<m, th, 0, c->stream>>>(psi, count, c->d_chunks);
+    scan_chunks_kernel<<<1, 1024, 0, c->stream>>>(c->d_chunks, m);
+    sample_kernel<Planar64><<<sblocks, th, 0, c->stream>>>(psi, count, c->d_chunks, m, d_rand, shots, d_out);
+  } else if (c->last_prec == BK_C64) {
     auto psi = reinterpret_cast<const float2*>(c->d_state);
     chunk_sums_kernel<float2><<<m, th, 0, c->stream>>>(psi, count, c->d_chunks);
     scan_chunks_kernel<<<1, 1024, 0, c->stream>>>(c->d_chunks, m);

@@ -1,0 +1,698 @@
+// Persistent dataflow engine (sm_100a): every Trotter step of one or many
+// statevectors in ONE launch, scheduled as tile tasks with dependency counters.
+//
+// Elements. The tile machinery works on 16-byte elements: a complex128
+// amplitude, or a PAIR of complex64 amplitudes stored pair-planar as
+// (re[2k], re[2k+1], im[2k], im[2k+1]) so that packed f32x2 FMAs act on
+// (re, re) and (im, im) register pairs. A tile is 4096 elements (64 KB); element
+// bit b is amplitude bit b (complex128) or b + 1 (complex64, whose amplitude
+// bit 0 lives inside the element).
+//
+// Tasks of one step (per statevector):
+//   A1  elements bits [0, 12): measurement (optional), diagonal phase D, Rx on
+//       the 12 element bits (+ amplitude bit 0 for complex64);
+//   S2  bits [0, 12 - W2) u [12, 12 + W2): Rx on W2 high element bits;
+//   S3  bits [0, 12 - W3) u [12 + W2, n'): Rx on the remaining W3 bits;
+//   M   measurement only (after the last step).
+// Dependencies (cumulative counters, never reset inside a launch):
+//   S2 tile of slab h  <- all 2^W2 A1 tiles of slab h of the same step;
+//   S3 tile            <- all S2 tiles of the statevector and step;
+//   A1 of step k + 1   <- all S3 (or, without S3, all S2) tiles of step k.
+// The task order interleaves A1 of slab h + 1 before S2 of slab h, so a slab
+// written by A1 is re-read by S2 while it is still in L2: A1 + S2 together cost
+// one HBM round trip.
+//
+// CTA = 8 compute warps + 1 producer warp. The producer claims tasks from a
+// global counter (in order, so every dependency points to an earlier task held
+// by a running CTA: no deadlock), waits (bounded) for the dependency, and TMA-
+// loads the tile into one of two shared-memory stages; the compute warps work
+// on the other stage. All waits are bounded and a global abort word stops every
+// CTA after the first failure.
+#pragma once
+#include "bk_device.cuh"
+#include "bk_fused.cuh"
+
+namespace bk {
+
+constexpr int kElemBits = 12;          // 4096 elements per tile
+constexpr int kStageTileBytes = 65536;
+constexpr int kStageEBytes = 16384;    // A1: uint16 E of 8192 (c64) / 4096 (c128) amplitudes
+constexpr int kStages = 2;
+constexpr int kComputeThreads = 256;
+constexpr int kPersistThreads = kComputeThreads + 32;
+
+enum TaskKind : int { TASK_A1 = 0, TASK_S2 = 1, TASK_S3 = 2, TASK_M = 3, TASK_END = 7 };
+
+// ---------------------------------------------------------------------------
+// element types
+// ---------------------------------------------------------------------------
+template <class R>
+struct El;
+
+template <>
+struct El<float> {
+  struct T {
+    float2 re, im;  // amplitudes 2k (x) and 2k + 1 (y)
+  };
+  static constexpr int kAmps = 2;
+  __device__ static T ld(const void* p) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    return T{make_float2(q.x, q.y), make_float2(q.z, q.w)};
+  }
+  __device__ static void st(void* p, const T& v) {
+    *reinterpret_cast<float4*>(p) = make_float4(v.re.x, v.re.y, v.im.x, v.im.y);
+  }
+  // a' = a + i t b, b' = b + i t a on both amplitudes of the elements at once
+  __device__ static void bfly(T& a, T& b, float t) {
+    const float2 pt = make_float2(t, t), nt = make_float2(-t, -t);
+    const T x = a, y = b;
+    a.re = __ffma2_rn(nt, y.im, x.re);
+    a.im = __ffma2_rn(pt, y.re, x.im);
+    b.re = __ffma2_rn(nt, x.im, y.re);
+    b.im = __ffma2_rn(pt, x.re, y.im);
+  }
+  // the butterfly between the two amplitudes inside the element (amplitude bit 0)
+  __device__ static void bfly_inner(T& a, float t) {
+    const T x = a;
+    a.re.x = fmaf(-t, x.im.y, x.re.x);
+    a.im.x = fmaf(t, x.re.y, x.im.x);
+    a.re.y = fmaf(-t, x.im.x, x.re.y);
+    a.im.y = fmaf(t, x.re.x, x.im.y);
+  }
+  __device__ static T shfl_xor(const T& v, int m) {
+    T r;
+    r.re.x = __shfl_xor_sync(0xffffffffu, v.re.x, m);
+    r.re.y = __shfl_xor_sync(0xffffffffu, v.re.y, m);
+    r.im.x = __shfl_xor_sync(0xffffffffu, v.im.x, m);
+    r.im.y = __shfl_xor_sync(0xffffffffu, v.im.y, m);
+    return r;
+  }
+  __device__ static void bfly_partner(T& a, const T& b, float t) {
+    const float2 pt = make_float2(t, t), nt = make_float2(-t, -t);
+    const T x = a;
+    a.re = __ffma2_rn(nt, b.im, x.re);
+    a.im = __ffma2_rn(pt, b.re, x.im);
+  }
+  __device__ static void scale(T& a, float s) {
+    const float2 ss = make_float2(s, s);
+    a.re = __fmul2_rn(a.re, ss);
+    a.im = __fmul2_rn(a.im, ss);
+  }
+};
+
+template <>
+struct El<double> {
+  struct T {
+    double2 v;
+  };
+  static constexpr int kAmps = 1;
+  __device__ static T ld(const void* p) { return T{*reinterpret_cast<const double2*>(p)}; }
+  __device__ static void st(void* p, const T& v) { *reinterpret_cast<double2*>(p) = v.v; }
+  __device__ static void bfly(T& a, T& b, double t) { bk::bfly(a.v, b.v, t); }
+  __device__ static void bfly_inner(T&, double) {}
+  __device__ static T shfl_xor(const T& v, int m) {
+    T r;
+    r.v.x = __shfl_xor_sync(0xffffffffu, v.v.x, m);
+    r.v.y = __shfl_xor_sync(0xffffffffu, v.v.y, m);
+    return r;
+  }
+  __device__ static void bfly_partner(T& a, const T& b, double t) { bk::bfly_partner(a.v, b.v, t); }
+  __device__ static void scale(T& a, double s) {
+    a.v.x *= s;
+    a.v.y *= s;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// diagonal phase on an element. complex64: E = h K + l per amplitude, residual
+// rotation by polynomials and the level rotation hab[h] = {-tan(th_h/4),
+// sin(th_h/2)} applied twice (th_h reduced to (-pi, pi]); every rotation as
+// shears (determinant exactly 1), vectorised over the element's two amplitudes.
+// ---------------------------------------------------------------------------
+struct PhaseV32 {
+  const float2* hab;  // [n_h]
+  uint32_t K, M;      // h = umulhi(E, M)
+  float theta, theta_lo;
+  int n_h;
+};
+struct PhaseV64 {
+  const double2* hi;  // [n_hi] (cos, sin)(theta 128 h)
+  const double2* lo;  // [128]  (cos, sin)(theta l)
+  int n_hi;
+};
+template <class R>
+struct PhaseV;
+template <>
+struct PhaseV<float> {
+  using params = PhaseV32;
+  static constexpr int kSmemBytes = kPhaseH * (int)sizeof(float2);
+  __device__ static void stage(const PhaseV32& P, unsigned char* s, int tid, int nthr) {
+    float2* hab = reinterpret_cast<float2*>(s);
+    for (int i = tid; i < P.n_h; i += nthr) hab[i] = P.hab[i];
+  }
+  __device__ static void shear2(float2& x, float2& y, float2 a, float2 b) {
+    x = __ffma2_rn(a, y, x);
+    y = __ffma2_rn(b, x, y);
+    x = __ffma2_rn(a, y, x);
+  }
+  __device__ static void apply(El<float>::T& v, uint32_t e2, const PhaseV32& P, const unsigned char* s,
+                               bool inverse) {
+    const float2* hab = reinterpret_cast<const float2*>(s);
+    const uint32_t e0 = e2 & 0xFFFFu, e1 = e2 >> 16;
+    const uint32_t h0 = __umulhi(e0, P.M), h1 = __umulhi(e1, P.M);
+    const uint32_t l0 = e0 - h0 * P.K, l1 = e1 - h1 * P.K;
+    const float2 lf = __fadd2_rn(make_float2(__int_as_float(0x4B000000 | l0), __int_as_float(0x4B000000 | l1)),
+                                 make_float2(-8388608.0f, -8388608.0f));
+    const float2 r = __ffma2_rn(lf, make_float2(P.theta, P.theta), __fmul2_rn(lf, make_float2(P.theta_lo, P.theta_lo)));
+    // a = -tan(r/2), b = sin r (Maclaurin to degree 9; |r| <= 1/2)
+    const float2 x = __fmul2_rn(r, make_float2(0.5f, 0.5f));
+    const float2 x2 = __fmul2_rn(x, x);
+    float2 tt = __ffma2_rn(x2, make_float2(62.0f / 2835.0f, 62.0f / 2835.0f), make_float2(17.0f / 315.0f, 17.0f / 315.0f));
+    tt = __ffma2_rn(x2, tt, make_float2(2.0f / 15.0f, 2.0f / 15.0f));
+    tt = __ffma2_rn(x2, tt, make_float2(1.0f / 3.0f, 1.0f / 3.0f));
+    tt = __ffma2_rn(x2, tt, make_float2(1.0f, 1.0f));
+    float2 a = __fmul2_rn(make_float2(-x.x, -x.y), tt);
+    const float2 r2 = __fmul2_rn(r, r);
+    float2 u = __ffma2_rn(r2, make_float2(1.0f / 362880.0f, 1.0f / 362880.0f), make_float2(-1.0f / 5040.0f, -1.0f / 5040.0f));
+    u = __ffma2_rn(r2, u, make_float2(1.0f / 120.0f, 1.0f / 120.0f));
+    u = __ffma2_rn(r2, u, make_float2(-1.0f / 6.0f, -1.0f / 6.0f));
+    u = __ffma2_rn(r2, u, make_float2(1.0f, 1.0f));
+    float2 b = __fmul2_rn(r, u);
+    const float2 H0 = hab[h0], H1 = hab[h1];
+    float2 A = make_float2(H0.x, H1.x), B = make_float2(H0.y, H1.y);
+    if (!inverse) {
+      shear2(v.re, v.im, a, b);
+      shear2(v.re, v.im, A, B);
+      shear2(v.re, v.im, A, B);
+    } else {
+      // inverse: the same shears with negated coefficients in reverse order
+      A = make_float2(-A.x, -A.y);
+      B = make_float2(-B.x, -B.y);
+      a = make_float2(-a.x, -a.y);
+      b = make_float2(-b.x, -b.y);
+      shear2(v.re, v.im, A, B);
+      shear2(v.re, v.im, A, B);
+      shear2(v.re, v.im, a, b);
+    }
+  }
+};
+template <>
+struct PhaseV<double> {
+  using params = PhaseV64;
+  static constexpr int kSmemBytes = (kPhaseHi64 + kPhaseLo) * (int)sizeof(double2);
+  __device__ static void stage(const PhaseV64& P, unsigned char* s, int tid, int nthr) {
+    double2* hi = reinterpret_cast<double2*>(s);
+    double2* lo = hi + kPhaseHi64;
+    for (int i = tid; i < P.n_hi; i += nthr) hi[i] = P.hi[i];
+    for (int i = tid; i < kPhaseLo; i += nthr) lo[i] = P.lo[i];
+  }
+  __device__ static void apply(El<double>::T& v, uint32_t e, const PhaseV64&, const unsigned char* s,
+                               bool inverse) {
+    const double2* hi = reinterpret_cast<const double2*>(s);
+    const double2* lo = hi + kPhaseHi64;
+    const double2 h = hi[e >> kPhaseLoBits], l = lo[e & (kPhaseLo - 1)];
+    const double c = fma(h.x, l.x, -h.y * l.y);
+    const double sn = inverse ? -fma(h.x, l.y, h.y * l.x) : fma(h.x, l.y, h.y * l.x);
+    v.v = make_double2(fma(v.v.x, c, -v.v.y * sn), fma(v.v.x, sn, v.v.y * c));
+  }
+};
+
+// ---------------------------------------------------------------------------
+// per-statevector descriptor (device memory) and the launch's task program
+// ---------------------------------------------------------------------------
+template <class R>
+struct InstDesc {
+  unsigned char* state;          // 16-byte elements
+  const CUtensorMap* map_a1;     // A1 / M tiles
+  const CUtensorMap* map_e;      // E tile of an A1 task
+  const CUtensorMap* map_s2;
+  const CUtensorMap* map_s3;
+  int np;                        // element bits (n for c128, n - 1 for c64)
+  int n;                         // qubits
+  int w2, w3;                    // widths of S2 / S3 (w3 = 0: no S3)
+  int a1_hi_dim;
+  int s2_mid_dim, s2_hi_dim, s2_mid_bits;
+  int s3_mid_dim, s3_hi_dim, s3_mid_bits;
+  int e0;
+  uint32_t s0;
+  typename PhaseV<R>::params phase;
+  const R* tan;                  // [n_steps]
+  const R* scale;                // [n_steps]: exact power of two applied with D
+  const int* slot;               // [n_steps + 1]: measurement row or -1
+  unsigned int* a1_done;         // [2^(np - 12 - w2)] per slab
+  unsigned int* s2_done;
+  unsigned int* s3_done;
+  unsigned int* ticket;
+  double* partials;              // [A1 tiles][3]
+  double* results;               // [rows][4]
+  uint32_t n_a1, n_s2, n_s3;     // tiles per step
+  int inverse;                   // reserved
+};
+
+struct Program {
+  const unsigned long long* tasks;  // one step's tasks: kind << 56 | inst << 32 | tile
+  uint32_t per_step;
+  uint32_t n_steps;
+  const unsigned long long* final_tasks;  // measurement-only tasks after the last step
+  uint32_t n_final;
+  uint32_t step0;                   // global step index of this launch's first step
+  unsigned int* next;               // work counter
+  int* err;
+  int* abort;
+};
+
+__device__ __forceinline__ uint32_t ld_acquire(const unsigned int* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void compute_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kComputeThreads) : "memory");
+}
+__device__ __forceinline__ bool aborted(const int* abort) {
+  return *reinterpret_cast<const volatile int*>(abort) != 0;
+}
+__device__ __forceinline__ void raise_error(const Program& P, int code) {
+  atomicCAS(P.err, 0, code);
+  atomicExch(P.abort, 1);
+}
+// bounded wait on an mbarrier phase that also gives up on a global abort
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t bar, uint32_t parity, const Program& P) {
+  for (uint32_t i = 0; i < kWaitPolls; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255u) == 255u && aborted(P.abort)) return false;
+  }
+  raise_error(P, DEV_TIMEOUT);
+  return false;
+}
+
+struct StageMeta {
+  int kind, inst;
+  uint32_t tile, step;
+};
+
+// ---------------------------------------------------------------------------
+// tile processing (compute warps; tid in [0, 256))
+// ---------------------------------------------------------------------------
+template <class R, uint32_t REG, bool SWZ>
+__device__ __forceinline__ void el_load(const unsigned char* s, typename El<R>::T (&v)[16], uint32_t base) {
+  const uint32_t sb = SWZ ? swz<double>(base) : base;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const uint32_t o = SWZ ? swz<double>(pdep((uint32_t)j, REG)) : pdep((uint32_t)j, REG);
+    v[j] = El<R>::ld(s + 16u * (sb ^ o));
+  }
+}
+template <class R, uint32_t REG>
+__device__ __forceinline__ void el_store_swz(unsigned char* s, const typename El<R>::T (&v)[16], uint32_t base) {
+  const uint32_t sb = swz<double>(base);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) El<R>::st(s + 16u * (sb ^ swz<double>(pdep((uint32_t)j, REG))), v[j]);
+}
+template <class R, uint32_t REG, uint32_t ACT>
+__device__ __forceinline__ void el_bflys(typename El<R>::T (&v)[16], R t) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if ((ACT & pdep(1u << k, REG)) != 0u) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (!(j & (1 << k))) El<R>::bfly(v[j], v[j | (1 << k)], t);
+    }
+  }
+}
+template <class R, uint32_t REG, int CP>
+__device__ __forceinline__ void el_gstore(unsigned char* g, const typename El<R>::T (&v)[16], uint32_t tile_base,
+                                          uint32_t base, uint32_t h0) {
+  const uint32_t gb = tile_base | tile_to_global<CP>(base, h0);
+#pragma unroll
+  for (int j = 0; j < 16; ++j)
+    El<R>::st(g + 16ull * (gb | tile_to_global<CP>(pdep((uint32_t)j, REG), h0)), v[j]);
+}
+
+// measurement helpers on an element with E (c64: two uint16 packed)
+__device__ __forceinline__ void measure_el(MeasureAcc& acc, const El<float>::T& v, uint32_t e2, uint32_t elem_g,
+                                           int e0, uint32_t s0) {
+  const uint32_t a0 = elem_g << 1;
+  acc.add((double)fmaf(v.re.x, v.re.x, v.im.x * v.im.x), (int)(e2 & 0xFFFFu) < e0, __popc(a0 ^ s0));
+  acc.add((double)fmaf(v.re.y, v.re.y, v.im.y * v.im.y), (int)(e2 >> 16) < e0, __popc((a0 | 1u) ^ s0));
+}
+__device__ __forceinline__ void measure_el(MeasureAcc& acc, const El<double>::T& v, uint32_t e, uint32_t elem_g,
+                                           int e0, uint32_t s0) {
+  acc.add(fma(v.v.x, v.v.x, v.v.y * v.v.y), (int)e < e0, __popc(elem_g ^ s0));
+}
+template <class R>
+__device__ __forceinline__ uint32_t load_e(const unsigned char* etile, uint32_t elem) {
+  if constexpr (sizeof(R) == 4)
+    return reinterpret_cast<const uint32_t*>(etile)[elem];
+  else
+    return reinterpret_cast<const uint16_t*>(etile)[elem];
+}
+
+// consumer-side block reduction: per-tile partials, last tile of the step
+// reduces all of them in index order into results[slot]
+__device__ __forceinline__ void compute_reduce(MeasureAcc acc, double* partials, unsigned int* ticket,
+                                               double* results, int slot, uint32_t tile, uint32_t ntiles,
+                                               double* red /* smem [3][8] */, int* last_flag) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double a = warp_sum(acc.norm), b = warp_sum(acc.p_less), c = warp_sum(acc.d_h);
+  if (lane == 0) {
+    red[0 * 8 + warp] = a;
+    red[1 * 8 + warp] = b;
+    red[2 * 8 + warp] = c;
+  }
+  compute_sync();
+  if (tid == 0) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int w = 0; w < 8; ++w) {
+      s0 += red[w];
+      s1 += red[8 + w];
+      s2 += red[16 + w];
+    }
+    partials[3 * (size_t)tile + 0] = s0;
+    partials[3 * (size_t)tile + 1] = s1;
+    partials[3 * (size_t)tile + 2] = s2;
+    __threadfence();
+    *last_flag = (atomicAdd(ticket, 1u) == ntiles - 1u);
+  }
+  compute_sync();
+  if (!*last_flag) return;
+  __threadfence();
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (uint32_t i = tid; i < ntiles; i += kComputeThreads) {
+    s0 += __ldcg(&partials[3 * (size_t)i + 0]);
+    s1 += __ldcg(&partials[3 * (size_t)i + 1]);
+    s2 += __ldcg(&partials[3 * (size_t)i + 2]);
+  }
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  s2 = warp_sum(s2);
+  compute_sync();
+  if (lane == 0) {
+    red[warp] = s0;
+    red[8 + warp] = s1;
+    red[16 + warp] = s2;
+  }
+  compute_sync();
+  if (tid == 0) {
+    double nn = 0, p = 0, d = 0;
+    for (int w = 0; w < 8; ++w) {
+      nn += red[w];
+      p += red[8 + w];
+      d += red[16 + w];
+    }
+    results[4 * (size_t)slot + 0] = p;
+    results[4 * (size_t)slot + 1] = d;
+    results[4 * (size_t)slot + 2] = nn;
+    *ticket = 0u;
+  }
+}
+
+// A1 (and measurement-only M) on a staged tile
+template <class R, bool MEASURE_ONLY>
+__device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned char* etile, const InstDesc<R>& D,
+                                           uint32_t t_idx, uint32_t step, const unsigned char* phase_smem,
+                                           double* red, int* last_flag) {
+  using PL = Plan<double>;
+  using E = El<R>;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t tile_base = t_idx << kElemBits;
+  typename E::T v[16];
+  const uint32_t b1 = pdep(lane, PL::A1_R1_LANE) | pdep(warp, PL::A1_R1_WARP);
+  el_load<R, PL::A1_R1_REG, false>(tile, v, b1);
+  const int slot = D.slot[step];
+  MeasureAcc acc;
+  const R t = MEASURE_ONLY ? (R)0 : D.tan[step];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const uint32_t i = b1 | pdep((uint32_t)j, PL::A1_R1_REG);
+    const uint32_t e = load_e<R>(etile, i);
+    if (MEASURE_ONLY || slot >= 0) measure_el(acc, v[j], e, tile_base | i, D.e0, D.s0);
+    if (!MEASURE_ONLY) {
+      PhaseV<R>::apply(v[j], e, D.phase, phase_smem, false);
+      E::bfly_inner(v[j], t);
+    }
+  }
+  if (!MEASURE_ONLY) {
+    const R sc = D.scale[step];
+    if (sc != (R)1) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) E::scale(v[j], sc);
+    }
+    el_bflys<R, PL::A1_R1_REG, PL::A1_R1_REG>(v, t);
+    compute_sync();
+    el_store_swz<R, PL::A1_R1_REG>(tile, v, b1);
+    compute_sync();
+    const uint32_t b2 = pdep(lane, PL::A1_R2_LANE) | pdep(warp, PL::A1_R2_WARP);
+    el_load<R, PL::A1_R2_REG, true>(tile, v, b2);
+    el_bflys<R, PL::A1_R2_REG, PL::A1_R2_REG>(v, t);
+    compute_sync();
+    el_store_swz<R, PL::A1_R2_REG>(tile, v, b2);
+    compute_sync();
+    const uint32_t b3 = pdep(lane, PL::A1_R3_LANE) | pdep(warp, PL::A1_R3_WARP);
+    el_load<R, PL::A1_R3_REG, true>(tile, v, b3);
+    el_bflys<R, PL::A1_R3_REG, PL::A1_R3_ACT>(v, t);
+    el_gstore<R, PL::A1_R3_REG, kElemBits>(D.state, v, tile_base, b3, 0);
+  }
+  if (MEASURE_ONLY || slot >= 0)
+    compute_reduce(acc, D.partials, D.ticket, D.results, MEASURE_ONLY ? D.slot[step] : slot, t_idx, D.n_a1, red,
+                   last_flag);
+}
+
+// strided pass of width W on a staged tile (element bits [0, 12 - W) u [h0, h0 + W))
+template <class R, int W>
+__device__ __forceinline__ void process_s(unsigned char* tile, unsigned char* state, uint32_t tile_base,
+                                          uint32_t h0, R t) {
+  using PL = Plan<double>;
+  using E = El<R>;
+  constexpr int CP = kElemBits - W;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  typename E::T v[16];
+  constexpr uint32_t ACT_ALL = ((1u << W) - 1u) << CP;
+  const uint32_t b1 = pdep(lane, PL::S_R1_LANE) | pdep(warp, PL::S_R1_WARP);
+  el_load<R, PL::S_R1_REG, false>(tile, v, b1);
+  el_bflys<R, PL::S_R1_REG, ACT_ALL>(v, t);
+  if constexpr (W <= 4) {
+    el_gstore<R, PL::S_R1_REG, CP>(state, v, tile_base, b1, h0);
+  } else {
+    using R2 = StridedR2<double, W>;
+    compute_sync();
+    el_store_swz<R, PL::S_R1_REG>(tile, v, b1);
+    compute_sync();
+    const uint32_t b2 = pdep(lane, R2::LANE) | pdep(warp, R2::WARP);
+    el_load<R, R2::REG, true>(tile, v, b2);
+    el_bflys<R, R2::REG, R2::ACT>(v, t);
+    if constexpr (R2::kShuffleLaneBit >= 0) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const typename E::T q = E::shfl_xor(v[j], 1 << R2::kShuffleLaneBit);
+        E::bfly_partner(v[j], q, t);
+      }
+    }
+    el_gstore<R, R2::REG, CP>(state, v, tile_base, b2, h0);
+  }
+}
+
+template <class R>
+__device__ __forceinline__ void process_s_dispatch(int w, unsigned char* tile, unsigned char* state,
+                                                   uint32_t tile_base, uint32_t h0, R t) {
+  switch (w) {
+    case 1: process_s<R, 1>(tile, state, tile_base, h0, t); break;
+    case 2: process_s<R, 2>(tile, state, tile_base, h0, t); break;
+    case 3: process_s<R, 3>(tile, state, tile_base, h0, t); break;
+    case 4: process_s<R, 4>(tile, state, tile_base, h0, t); break;
+    case 5: process_s<R, 5>(tile, state, tile_base, h0, t); break;
+    case 6: process_s<R, 6>(tile, state, tile_base, h0, t); break;
+    case 7: process_s<R, 7>(tile, state, tile_base, h0, t); break;
+    case 8: process_s<R, 8>(tile, state, tile_base, h0, t); break;
+    default: process_s<R, 9>(tile, state, tile_base, h0, t); break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the persistent kernel
+// ---------------------------------------------------------------------------
+struct PersistSmem {
+  static constexpr int kStageBytes = kStageTileBytes + kStageEBytes;
+  static constexpr int kMetaOff = kStages * kStageBytes;
+  static constexpr int kPhaseOff = kMetaOff + 256;
+  static constexpr int kRedOff = kPhaseOff + 3328;  // >= both phase table footprints
+  static constexpr int kBytes = kRedOff + 256;
+};
+
+template <class R>
+__global__ void __launch_bounds__(kPersistThreads, 1)
+    persist_kernel(const InstDesc<R>* __restrict__ insts, const Program P) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
+  __shared__ int last_flag;
+  __shared__ int cur_phase_inst;
+  StageMeta* meta = reinterpret_cast<StageMeta*>(smem + PersistSmem::kMetaOff);
+  unsigned char* phase_smem = smem + PersistSmem::kPhaseOff;
+  double* red = reinterpret_cast<double*>(smem + PersistSmem::kRedOff);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(smem_addr(&full_bar[s]), 1);
+      mbar_init(smem_addr(&empty_bar[s]), 1);
+    }
+    fence_barrier_init();
+    cur_phase_inst = -1;
+  }
+  __syncthreads();
+
+  const uint32_t total = P.per_step * P.n_steps + P.n_final;
+
+  if (tid >= kComputeThreads) {
+    // ------------------------------ producer ------------------------------
+    if (tid != kComputeThreads) return;
+    uint32_t use[kStages] = {0, 0};
+    int s = 0;
+    bool stop = false;
+    while (!stop) {
+      const uint32_t g = aborted(P.abort) ? total : atomicAdd(P.next, 1u);
+      StageMeta m;
+      uint32_t bytes = 0;
+      if (g >= total) {
+        m.kind = TASK_END;
+        stop = true;
+      } else {
+        unsigned long long task;
+        uint32_t k;
+        if (g < P.per_step * P.n_steps) {
+          k = g / P.per_step;
+          task = P.tasks[g - k * P.per_step];
+        } else {
+          k = P.n_steps;
+          task = P.final_tasks[g - P.per_step * P.n_steps];
+        }
+        m.kind = (int)(task >> 56);
+        m.inst = (int)((task >> 32) & 0xFFFFFFu);
+        m.tile = (uint32_t)task;
+        m.step = k;  // step index inside this launch
+      }
+      // wait for the stage to be free
+      if (use[s] > 0 && !mbar_wait_or_abort(smem_addr(&empty_bar[s]), (use[s] - 1u) & 1u, P)) {
+        m.kind = TASK_END;
+        stop = true;
+      }
+      if (m.kind != TASK_END) {
+        const InstDesc<R>& D = insts[m.inst];
+        // dependency
+        const unsigned int* ctr = nullptr;
+        uint32_t target = 0;
+        const uint32_t kk = m.step;
+        if (m.kind == TASK_A1 || m.kind == TASK_M) {
+          if (kk > 0) {
+            ctr = D.w3 > 0 ? D.s3_done : D.s2_done;
+            target = (D.w3 > 0 ? D.n_s3 : D.n_s2) * kk;
+          }
+        } else if (m.kind == TASK_S2) {
+          ctr = D.a1_done + (m.tile >> D.w2);
+          target = (1u << D.w2) * (kk + 1u);
+        } else {
+          ctr = D.s2_done;
+          target = D.n_s2 * (kk + 1u);
+        }
+        if (ctr) {
+          uint32_t polls = 0;
+          while (ld_acquire(ctr) < target) {
+            if (++polls > kWaitPolls * 4u) {
+              raise_error(P, DEV_TIMEOUT);
+              break;
+            }
+            if ((polls & 63u) == 0u && aborted(P.abort)) break;
+            __nanosleep(64);
+          }
+          if (aborted(P.abort)) {
+            m.kind = TASK_END;
+            stop = true;
+          }
+          fence_proxy_async_global();
+        }
+        if (m.kind != TASK_END) {
+          const uint32_t fb = smem_addr(&full_bar[s]);
+          unsigned char* dst = smem + s * PersistSmem::kStageBytes;
+          meta[s] = m;
+          if (m.kind == TASK_A1 || m.kind == TASK_M) {
+            bytes = kStageTileBytes + (uint32_t)(4096 * 2 * El<R>::kAmps);
+            mbar_arrive_expect_tx(fb, bytes);
+            const int hd = D.a1_hi_dim;
+            tma_load_5d(smem_addr(dst), D.map_a1, 0, 0, hd == 2 ? (int)m.tile : 0, hd == 3 ? (int)m.tile : 0, 0, fb);
+            tma_load_5d(smem_addr(dst + kStageTileBytes), D.map_e, 0, 0, (int)m.tile, 0, 0, fb);
+          } else {
+            const bool s2 = (m.kind == TASK_S2);
+            const int mb = s2 ? D.s2_mid_bits : D.s3_mid_bits;
+            const int md = s2 ? D.s2_mid_dim : D.s3_mid_dim;
+            const int hd = s2 ? D.s2_hi_dim : D.s3_hi_dim;
+            const int mid = (int)(m.tile & ((1u << mb) - 1u)), hi = (int)(m.tile >> mb);
+            bytes = kStageTileBytes;
+            mbar_arrive_expect_tx(fb, bytes);
+            tma_load_5d(smem_addr(dst), s2 ? D.map_s2 : D.map_s3, tile_coord(0, md, mid, hd, hi),
+                        tile_coord(1, md, mid, hd, hi), tile_coord(2, md, mid, hd, hi),
+                        tile_coord(3, md, mid, hd, hi), tile_coord(4, md, mid, hd, hi), fb);
+          }
+        }
+      }
+      if (m.kind == TASK_END) {
+        meta[s] = m;
+        mbar_arrive(smem_addr(&full_bar[s]));
+      }
+      ++use[s];
+      s ^= 1;
+    }
+    // let in-flight loads land before leaving (bounded)
+    for (int q = 0; q < kStages; ++q)
+      if (use[q] > 0) mbar_wait_bounded(smem_addr(&full_bar[q]), (use[q] - 1u) & 1u, P.err);
+    return;
+  }
+
+  // ------------------------------ consumers ------------------------------
+  int s = 0;
+  uint32_t use[kStages] = {0, 0};
+  for (;;) {
+    if (!mbar_wait_or_abort(smem_addr(&full_bar[s]), use[s] & 1u, P)) break;
+    const StageMeta m = meta[s];
+    if (m.kind == TASK_END) break;
+    const InstDesc<R>& D = insts[m.inst];
+    unsigned char* tile = smem + s * PersistSmem::kStageBytes;
+    if (m.kind == TASK_A1) {
+      if (cur_phase_inst != m.inst) {
+        compute_sync();
+        PhaseV<R>::stage(D.phase, phase_smem, tid, kComputeThreads);
+        compute_sync();
+        if (tid == 0) cur_phase_inst = m.inst;
+      }
+      process_a1<R, false>(tile, tile + kStageTileBytes, D, m.tile, m.step, phase_smem, red, &last_flag);
+    } else if (m.kind == TASK_M) {
+      process_a1<R, true>(tile, tile + kStageTileBytes, D, m.tile, m.step, phase_smem, red, &last_flag);
+    } else {
+      const bool s2 = (m.kind == TASK_S2);
+      const int w = s2 ? D.w2 : D.w3;
+      const int mb = s2 ? D.s2_mid_bits : D.s3_mid_bits;
+      const uint32_t h0 = s2 ? (uint32_t)kElemBits : (uint32_t)(kElemBits + D.w2);
+      const uint32_t cp = (uint32_t)(kElemBits - w);
+      const uint32_t mid = m.tile & ((1u << mb) - 1u), hi = m.tile >> mb;
+      const uint32_t tile_base = (mid << cp) | (hi << (h0 + (uint32_t)w));
+      process_s_dispatch<R>(w, tile, D.state, tile_base, h0, D.tan[m.step]);
+    }
+    // completion: stores visible gpu-wide, then count the task and free the stage
+    __threadfence();
+    compute_sync();
+    if (tid == 0) {
+      if (m.kind == TASK_A1) atomicAdd(D.a1_done + (m.tile >> D.w2), 1u);
+      else if (m.kind == TASK_S2) atomicAdd(D.s2_done, 1u);
+      else if (m.kind == TASK_S3) atomicAdd(D.s3_done, 1u);
+      mbar_arrive(smem_addr(&empty_bar[s]));
+    }
+    ++use[s];
+    s ^= 1;
+  }
+}
+
+}  // namespace bk

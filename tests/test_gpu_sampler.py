@@ -93,3 +93,30 @@ def test_d_min_matches_oracle(eng, golden):
     for n_s in ("26", "28", "30"):
         for r in golden("traps.json")["results"][n_s][::3]:
             assert eng.d_min(int(n_s), int(r["trap_bits"], 16), int(r["trap_energy"])) == int(r["d_min"])
+
+
+def test_sampling_segments_do_not_disturb_the_evolution(eng):
+    # complex64 n = 16 runs on the persistent engine, split into launches at the
+    # sampling points; the measured series must equal the unsampled run exactly
+    n = 16
+    bits = O.steepest_descent(n, int(O.random_states(n, 4, 1)[0]))[0]
+    common = dict(n=n, g=0.35, dt=0.05, t_max=2.0, track_p_less=True, verbose=False, precision=bk.BK_C64)
+    a = eng.sampler_run(bits, shots_per_point=0, t_start=0.0, dt_sample=0.05, num_sample_points=41, **common)
+    b = eng.sampler_run(bits, shots_per_point=64, t_start=0.5, dt_sample=0.25, num_sample_points=5, **common)
+    tb = np.round(b["time_points"] / 0.05).astype(int)
+    assert np.array_equal(a["p_less_history"][tb], b["p_less_history"])
+    assert b["total_shots_collected"] == 5 * 64
+
+
+def test_sampling_c64_planar_vs_c128(eng):
+    n = 16
+    bits = O.steepest_descent(n, int(O.random_states(n, 6, 1)[0]))[0]
+    kw = dict(n=n, g=0.35, dt=0.05, t_max=3.0, shots_per_point=200, t_start=1.0, dt_sample=0.5,
+              num_sample_points=5, num_sampling_seeds=2, verbose=False)
+    r64 = eng.sampler_run(bits, precision=bk.BK_C64, **kw)
+    r128 = eng.sampler_run(bits, precision=bk.BK_C128, **kw)
+    assert np.array_equal(r64["time_points"], r128["time_points"])
+    assert np.max(np.abs(r64["p_less_history"] - r128["p_less_history"])) <= 1e-6
+    # same uniforms, CDFs within complex64 rounding: nearly every draw identical
+    assert abs(r64["improved_shots"] - r128["improved_shots"]) <= 3
+    assert [s["total_shots_collected"] for s in r64["seed_stats"]] == [s["total_shots_collected"] for s in r128["seed_stats"]]
