@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--cpu-baseline-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--engine-mode", type=int, default=None, help="0 persistent, 1 one launch per pass")
+    ap.add_argument("--slab-lag", type=int, default=None)
     return ap.parse_args()
 
 
@@ -202,6 +204,10 @@ def main():
     n, T = a.n, a.trotter
     prec = bk.BK_C64 if a.precision == "c64" else bk.BK_C128
     eng = bk.Engine(local)
+    if a.engine_mode is not None:
+        eng.set_option("engine_mode", a.engine_mode)
+    if a.slab_lag is not None:
+        eng.set_option("slab_lag", a.slab_lag)
     bits, e0 = bk.select_trap(n, 42 + rank, 4000, 0.01)
     meas = list(range(0, T + 1, a.measure_every))
     dev = torch.device("cuda", local)
@@ -247,8 +253,12 @@ def main():
 
     # ---- roofline of the dominant kernel ----
     S = 8 if prec == bk.BK_C64 else 16
+    # algorithmic bytes per launch: a pass reads and writes the state once (2 S per
+    # amplitude); one persistent launch runs all T Trotter steps of a call (4 S per
+    # amplitude-step: two such passes per step)
     per_launch_bytes = {"a1_step": 2 * S, "a1_step_measure": 2 * S, "a1_measure": S, "measure": S,
-                        "plain_phase": 2 * S, "plain_rx": 2 * S}
+                        "plain_phase": 2 * S, "plain_rx": 2 * S, "persist": 4 * S * T,
+                        "tile_a1": 2 * S, "tile_s2": 2 * S, "tile_s3": 2 * S, "tile_m": S}
     dom = max(timing.items(), key=lambda kv: kv[1][1])
     dname, (dl, dms) = dom
     abytes = per_launch_bytes.get(dname, 2 * S) * float(1 << n)

@@ -36,6 +36,17 @@ class EvolveParams(ctypes.Structure):
                 ("reserved1", ctypes.c_int32), ("randnums", _dp), ("samples_out", _u64p)]
 
 
+class BatchInstanceC(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("reserved", ctypes.c_int32), ("s0", ctypes.c_uint64), ("e0", ctypes.c_int64),
+                ("g_const", ctypes.c_double), ("g", _dp)]
+
+
+class BatchParamsC(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int32), ("n_steps", ctypes.c_int32), ("dt", ctypes.c_double),
+                ("diag_scale", ctypes.c_double), ("measure", _u8p), ("use_graph", ctypes.c_int32),
+                ("lag", ctypes.c_int32)]
+
+
 class SamplerConfigC(ctypes.Structure):
     """bk_sampler_config — the reference's SamplerConfig (sampler.cuh:235-260) plus precision/method."""
     _fields_ = [("n", ctypes.c_int32), ("num_sample_points", ctypes.c_int32), ("shots_per_point", ctypes.c_int32),
@@ -101,6 +112,10 @@ def load_library(build_if_missing=True):
     L.bk_kernel_timing.argtypes = [c_ctx, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _i64p, _dp]
     L.bk_sample.argtypes = [c_ctx, _dp, ctypes.c_int64, _u64p]
     L.bk_stream.argtypes = [c_ctx, ctypes.POINTER(ctypes.c_void_p)]
+    L.bk_set_option.argtypes = [c_ctx, ctypes.c_int, ctypes.c_int64]
+    L.bk_evolve_batch.argtypes = [c_ctx, ctypes.POINTER(BatchParamsC), ctypes.POINTER(BatchInstanceC), ctypes.c_int32,
+                                  _dp, _dp, _dp]
+    L.bk_get_option.argtypes = [c_ctx, ctypes.c_int, _i64p]
     L.bk_sampler_run.argtypes = [c_ctx, ctypes.POINTER(SamplerConfigC), ctypes.c_uint64,
                                  ctypes.POINTER(SamplingResultC)]
     L.bk_sampling_result_release.argtypes = [ctypes.POINTER(SamplingResultC)]
@@ -230,6 +245,39 @@ class Engine:
                     "bk_evolve")
         return p, d, nn
 
+    def evolve_batch(self, instances, dt, n_steps, measure=None, precision=BK_C64, use_graph=True, lag=0,
+                     diag_scale=0.0):
+        """Many statevectors in one persistent launch.
+
+        ``instances``: sequence of dicts with n, s0 and either g (scalar) or a per-step
+        schedule; optional e0. Returns (p_less, d_h, norm) as [instance, measurement]."""
+        flags = np.zeros(n_steps + 1, dtype=np.uint8)
+        if measure is None:
+            flags[:] = 1
+        else:
+            flags[np.asarray(list(measure), dtype=np.int64)] = 1
+        arr = (BatchInstanceC * len(instances))()
+        keep = []
+        for i, d in enumerate(instances):
+            arr[i].n = d["n"]
+            arr[i].s0 = d["s0"]
+            arr[i].e0 = d.get("e0", -1)
+            g = d.get("g", 0.35)
+            if np.ndim(g) == 0:
+                arr[i].g_const = float(g)
+            else:
+                ga = np.ascontiguousarray(g, dtype=np.float64)
+                keep.append(ga)
+                arr[i].g = _p(ga, _dp)
+        bp = BatchParamsC(precision=precision, n_steps=n_steps, dt=dt, diag_scale=diag_scale,
+                          measure=_p(flags, _u8p), use_graph=1 if use_graph else 0, lag=lag)
+        m = int(flags.sum())
+        shape = (len(instances), m)
+        p, d, nn = np.zeros(shape), np.zeros(shape), np.zeros(shape)
+        self._check(self.L.bk_evolve_batch(self.ctx, ctypes.byref(bp), arr, len(instances), _p(p, _dp), _p(d, _dp),
+                                           _p(nn, _dp)), "bk_evolve_batch")
+        return p, d, nn
+
     def d_min(self, n, bits, target=-1, max_d=-1):
         d = ctypes.c_int()
         self._check(self.L.bk_d_min(self.ctx, n, bits, target, max_d, ctypes.byref(d)), "bk_d_min")
@@ -278,6 +326,16 @@ class Engine:
         out = np.empty(len(r), dtype=np.uint64)
         self._check(self.L.bk_sample(self.ctx, _p(r, _dp), len(r), _p(out, _u64p)), "bk_sample")
         return out
+
+    OPTIONS = {"engine_mode": 0, "slab_lag": 1}
+
+    def set_option(self, name, value):
+        self._check(self.L.bk_set_option(self.ctx, self.OPTIONS[name], int(value)), "bk_set_option")
+
+    def get_option(self, name):
+        v = ctypes.c_int64()
+        self._check(self.L.bk_get_option(self.ctx, self.OPTIONS[name], ctypes.byref(v)), "bk_get_option")
+        return int(v.value)
 
     def stream_handle(self):
         """The engine's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""

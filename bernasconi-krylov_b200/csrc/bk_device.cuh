@@ -87,6 +87,37 @@ __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
+// Same load with an L2 cache-policy hint (createpolicy): streaming tiles are
+// loaded evict-first so they do not displace data that is about to be re-read.
+__device__ __forceinline__ void tma_load_5d_hint(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                                 int c3, int c4, uint32_t bar, uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7], %8;" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar), "l"(policy)
+      : "memory");
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// 16-byte global stores with an L2 cache-policy hint
+__device__ __forceinline__ void st_global_hint(void* p, float4 v, uint64_t policy) {
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z),
+               "f"(v.w), "l"(policy)
+               : "memory");
+}
+__device__ __forceinline__ void st_global_hint(void* p, double2 v, uint64_t policy) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v.x), "d"(v.y), "l"(policy)
+               : "memory");
+}
+
 // LABS energy (reference: src/labs_energy/labs_energy.hpp:121-132, and the device
 // form src/sampling/sampler.cuh:54-70), exact in integers.
 __device__ __forceinline__ int labs_energy(uint32_t x, int n) {

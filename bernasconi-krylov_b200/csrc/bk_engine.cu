@@ -86,6 +86,15 @@ struct bk_ctx {
   size_t persist_cap = 0;
   int num_sms = 148;
   bool planar = false;        // complex64 state stored pair-planar (persistent engine)
+  int slab_lag = 3;           // persistent engine: S2 queue lag behind A1, in slabs
+  int engine_mode = 0;        // 0 persistent dataflow, 1 one launch per pass (tile grid)
+  std::map<int, uint16_t*> batch_E;  // E tables of batched runs, per n
+  void* d_batch_state = nullptr;
+  size_t batch_state_cap = 0;
+  void* d_batch = nullptr;    // batched run: maps, descriptors, tasks, tables, counters, partials
+  size_t batch_cap = 0;
+  double* d_batch_results = nullptr;
+  size_t batch_results_cap = 0;
   // tensor maps, keyed by (state ptr, n, precision, pass)
   std::map<std::string, TmaDesc> tma;
   // last evolution (for export / sampling)
@@ -393,6 +402,68 @@ int build_phase(bk_ctx* c, int n, double angle_unit, Phase64* P) {
 
 bool is_finite(double x) { return std::isfinite(x); }
 
+// ---- trap generation (host) ----
+static int64_t host_energy(int n, uint64_t x) {
+  int64_t e = 0;
+  for (int k = 1; k < n; ++k) {
+    const int64_t ck = (int64_t)(n - k) - 2 * (int64_t)__builtin_popcountll((x ^ (x >> k)) & ((1ull << (n - k)) - 1ull));
+    e += ck * ck;
+  }
+  return e;
+}
+
+// Optimal LABS energies E*(n) for n <= 32 (reference: labs_energy.hpp:156-168).
+static int64_t optimal_energy(int n) {
+  static const int64_t t[33] = {-1, -1, -1, 1, 2, 2, 7, 3, 8, 12, 13, 5, 10, 6, 19, 15, 24,
+                                32, 25, 29, 26, 26, 39, 47, 36, 36, 45, 37, 50, 62, 59, 67, 64};
+  return (n >= 0 && n <= 32) ? t[n] : -1;
+}
+
+// One descent with incremental C_k (reference: classical.cuh:625-712). Each
+// sweep costs n evaluations; a flip is taken only when strictly better, the
+// lowest bit index winning ties.
+static void descend(int n, uint64_t start, uint64_t max_evals, uint64_t* fs, int64_t* fe, uint64_t* ev) {
+  const uint64_t budget = max_evals == 0 ? ~0ull : max_evals;
+  uint64_t x = start;
+  int64_t C[64];
+  int64_t e = 0;
+  for (int k = 1; k < n; ++k) {
+    C[k] = (int64_t)(n - k) - 2 * (int64_t)__builtin_popcountll((x ^ (x >> k)) & ((1ull << (n - k)) - 1ull));
+    e += C[k] * C[k];
+  }
+  uint64_t evals = 1;
+  while (evals + (uint64_t)n <= budget) {
+    int best = -1;
+    int64_t best_e = e;
+    for (int p = 0; p < n; ++p) {
+      const int sp = ((x >> p) & 1ull) ? -1 : 1;
+      int64_t ne = 0;
+      for (int k = 1; k < n; ++k) {
+        int64_t d = 0;
+        if (p + k < n) d -= 2 * sp * (((x >> (p + k)) & 1ull) ? -1 : 1);
+        if (p - k >= 0) d -= 2 * sp * (((x >> (p - k)) & 1ull) ? -1 : 1);
+        ne += (C[k] + d) * (C[k] + d);
+      }
+      if (ne < best_e) {
+        best_e = ne;
+        best = p;
+      }
+    }
+    evals += (uint64_t)n;
+    if (best < 0) break;
+    const int sp = ((x >> best) & 1ull) ? -1 : 1;
+    for (int k = 1; k < n; ++k) {
+      if (best + k < n) C[k] -= 2 * sp * (((x >> (best + k)) & 1ull) ? -1 : 1);
+      if (best - k >= 0) C[k] -= 2 * sp * (((x >> (best - k)) & 1ull) ? -1 : 1);
+    }
+    x ^= 1ull << best;
+    e = best_e;
+  }
+  *fs = x;
+  *fe = e;
+  if (ev) *ev = evals;
+}
+
 struct Schedule {
   std::vector<double> g;        // per step
   std::vector<int> slot;        // per step (n_steps + 1): measurement row or -1
@@ -560,11 +631,15 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
   auto task = [](int kind, int inst, uint32_t tile) {
     return ((unsigned long long)kind << 56) | ((unsigned long long)inst << 32) | tile;
   };
-  for (uint32_t h = 0; h <= slabs; ++h) {
+  // S2 of slab h is queued `lag` slabs after A1 of slab h: far enough behind the
+  // ~2 tasks per CTA in flight that the slab is finished, close enough that its
+  // data is still in L2 (lag x slab bytes of dirty lines)
+  const uint32_t lag = std::max<uint32_t>(1u, std::min<uint32_t>(slabs, (uint32_t)c->slab_lag));
+  for (uint32_t h = 0; h < slabs + lag; ++h) {
     if (h < slabs)
       for (uint32_t j = 0; j < per_slab; ++j) tasks.push_back(task(TASK_A1, 0, h * per_slab + j));
-    if (h > 0)
-      for (uint32_t j = 0; j < per_slab; ++j) tasks.push_back(task(TASK_S2, 0, (h - 1) * per_slab + j));
+    if (h >= lag)
+      for (uint32_t j = 0; j < per_slab; ++j) tasks.push_back(task(TASK_S2, 0, (h - lag) * per_slab + j));
   }
   for (uint32_t j = 0; j < n_s3; ++j) tasks.push_back(task(TASK_S3, 0, j));
   std::vector<unsigned long long> final_tasks;
@@ -646,6 +721,48 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
     BK_CUDA(c, cudaMemcpyAsync(base + o_hab, hab.data(), hab.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
   BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R>), PersistSmem::kBytes));
 
+  if (c->engine_mode == 1) {
+    // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_pass_kernel<R>), PersistSmem::kBytes));
+    using SampT = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
+    BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &D, sizeof(D), cudaMemcpyHostToDevice, st));
+    BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
+    const InstDesc<R>* dd = reinterpret_cast<const InstDesc<R>*>(base + o_desc);
+    for (int k = 0; k <= p->n_steps; ++k) {
+      if (S.sample_pt[(size_t)k] >= 0)
+        BK_TRY(launch_sampling_t(c, reinterpret_cast<const SampT*>(c->d_state), n, S.sample_pt[(size_t)k], S.shots));
+      size_t ev = 0;
+      if (k == p->n_steps) {
+        if (S.slot[(size_t)k] >= 0) {
+          BK_TRY(ev_begin(c, "tile_m", &ev));
+          tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(dd, TASK_M, (uint32_t)k, err);
+          BK_CUDA(c, cudaGetLastError());
+          BK_TRY(ev_end(c, ev));
+        }
+        break;
+      }
+      BK_TRY(ev_begin(c, "tile_a1", &ev));
+      tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(dd, TASK_A1, (uint32_t)k, err);
+      BK_CUDA(c, cudaGetLastError());
+      BK_TRY(ev_end(c, ev));
+      BK_TRY(ev_begin(c, "tile_s2", &ev));
+      tile_pass_kernel<R><<<n_s2, kComputeThreads, PersistSmem::kBytes, st>>>(dd, TASK_S2, (uint32_t)k, err);
+      BK_CUDA(c, cudaGetLastError());
+      BK_TRY(ev_end(c, ev));
+      if (n_s3 > 0) {
+        BK_TRY(ev_begin(c, "tile_s3", &ev));
+        tile_pass_kernel<R><<<n_s3, kComputeThreads, PersistSmem::kBytes, st>>>(dd, TASK_S3, (uint32_t)k, err);
+        BK_CUDA(c, cudaGetLastError());
+        BK_TRY(ev_end(c, ev));
+      }
+    }
+    int e = 0;
+    BK_CUDA(c, cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BK_CUDA(c, cudaStreamSynchronize(st));
+    if (e != 0) return fail(c, BK_ERR_TIMEOUT, "tile pass: a bounded device wait gave up (%d)", e);
+    return BK_OK;
+  }
+
   // one launch per segment between sampling points (sampling reads psi_k before step k)
   using Samp = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
   int k0 = 0, search = 0;
@@ -673,7 +790,7 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
     if (P.n_steps > 0 || P.n_final > 0) {
       size_t ev = 0;
       BK_TRY(ev_begin(c, "persist", &ev));
-      persist_kernel<R><<<c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
+      persist_kernel<R><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
           reinterpret_cast<const InstDesc<R>*>(base + o_desc), P);
       BK_CUDA(c, cudaGetLastError());
       BK_TRY(ev_end(c, ev));
@@ -695,7 +812,7 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
         P.n_final = (uint32_t)final_tasks.size();
         size_t ev = 0;
         BK_TRY(ev_begin(c, "persist", &ev));
-        persist_kernel<R><<<c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
+        persist_kernel<R><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
             reinterpret_cast<const InstDesc<R>*>(base + o_desc), P);
         BK_CUDA(c, cudaGetLastError());
         BK_TRY(ev_end(c, ev));
@@ -707,6 +824,339 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
     search = k1 + 1;
     // the next segment starts at k1; its first A1 measures step k1 if flagged
   }
+  return BK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batched evolution (persistent engine over many statevectors)
+// ---------------------------------------------------------------------------
+int batch_energy(bk_ctx* c, int n, uint16_t** out) {
+  auto it = c->batch_E.find(n);
+  if (it != c->batch_E.end()) {
+    *out = it->second;
+    return BK_OK;
+  }
+  uint16_t* d = nullptr;
+  const size_t count = 1ull << n;
+  BK_CUDA(c, cudaMalloc(&d, std::max<size_t>(count, 8) * sizeof(uint16_t)));
+  const uint32_t per = (uint32_t)((count + 7) / 8);
+  energy_table_kernel<<<(per + 255) / 256, 256, 0, c->stream>>>(d, n, (uint32_t)count);
+  BK_CUDA(c, cudaGetLastError());
+  c->batch_E[n] = d;
+  *out = d;
+  return BK_OK;
+}
+
+__global__ void set_basis_many_kernel(unsigned char* base, const unsigned long long* offsets,
+                                      const unsigned int* idx, int planar, int n_inst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_inst) return;
+  unsigned char* st = base + offsets[i];
+  const uint32_t s = idx[i];
+  if (planar)
+    reinterpret_cast<float*>(st)[4u * (s >> 1) + (s & 1u)] = 1.0f;
+  else
+    reinterpret_cast<double2*>(st)[s] = make_double2(1.0, 0.0);
+}
+
+template <class R>
+int evolve_batch_t(bk_ctx* c, const bk_batch_params* bp, const bk_batch_instance* inst, int n_inst,
+                   double* p_less, double* d_h, double* norm_out) {
+  const bool c64 = sizeof(R) == 4;
+  const int T = bp->n_steps;
+  std::vector<int> slot((size_t)T + 1, -1);
+  int n_meas = 0;
+  for (int k = 0; k <= T; ++k)
+    if (bp->measure == nullptr || bp->measure[k]) slot[(size_t)k] = n_meas++;
+  if (n_meas > 0 && (!p_less || !d_h)) return fail(c, BK_ERR_INVALID, "output arrays are NULL");
+
+  struct Geo {
+    int n, np, w2, w3, e0;
+    uint32_t n_a1, slabs, s0;
+    size_t state_off;
+    double angle_unit;
+  };
+  std::vector<Geo> geo((size_t)n_inst);
+  size_t state_bytes = 0;
+  for (int i = 0; i < n_inst; ++i) {
+    const bk_batch_instance& b = inst[i];
+    Geo g{};
+    g.n = b.n;
+    g.np = c64 ? b.n - 1 : b.n;
+    if (g.np <= kElemBits || b.n > kMaxN)
+      return fail(c, BK_ERR_UNSUPPORTED, "batched instance %d: n = %d outside [%d, %d]", i, b.n,
+                  kElemBits + (c64 ? 2 : 1), kMaxN);
+    const int rest = g.np - kElemBits;
+    g.w2 = (rest <= 9) ? rest : (rest + 1) / 2;
+    g.w3 = rest - g.w2;
+    if (g.w2 > 9 || g.w3 > 9) return fail(c, BK_ERR_UNSUPPORTED, "n = %d needs more than two strided passes", b.n);
+    g.n_a1 = 1u << (g.np - kElemBits);
+    g.slabs = 1u << (g.np - kElemBits - g.w2);
+    g.s0 = (uint32_t)(b.s0 & ((1ull << b.n) - 1ull));
+    int64_t e0 = b.e0;
+    if (e0 < 0) e0 = host_energy(b.n, g.s0);
+    g.e0 = (int)e0;
+    g.angle_unit = (bp->diag_scale > 0.0) ? bp->dt * bp->diag_scale : bp->dt / (double)b.n;
+    g.state_off = state_bytes;
+    state_bytes += (1ull << b.n) * (c64 ? 8 : 16);
+    geo[(size_t)i] = g;
+    if (b.g == nullptr && !is_finite(b.g_const)) return fail(c, BK_ERR_INVALID, "instance %d: g not finite", i);
+  }
+  BK_TRY(ensure_buffer(c, &c->d_batch_state, &c->batch_state_cap, state_bytes));
+  BK_TRY(ensure_buffer(c, reinterpret_cast<void**>(&c->d_batch_results), &c->batch_results_cap,
+                       std::max<size_t>((size_t)n_inst * n_meas * 4, 1) * sizeof(double)));
+  unsigned char* state = static_cast<unsigned char*>(c->d_batch_state);
+
+  // per-instance schedules of tangents, exact rescales and the log2 of the omitted factors
+  std::vector<R> tans((size_t)n_inst * std::max(T, 1)), scales((size_t)n_inst * std::max(T, 1));
+  std::vector<long double> row_log2((size_t)n_inst * std::max(n_meas, 1), 0.0L);
+  for (int i = 0; i < n_inst; ++i) {
+    long double lg = 0.0L;
+    for (int k = 0; k <= T; ++k) {
+      if (slot[(size_t)k] >= 0) row_log2[(size_t)i * n_meas + slot[(size_t)k]] = lg;
+      if (k == T) break;
+      const double gk = inst[i].g ? inst[i].g[k] : inst[i].g_const;
+      if (!is_finite(gk)) return fail(c, BK_ERR_INVALID, "instance %d: g[%d] not finite", i, k);
+      const R tf = (R)std::tan(gk * bp->dt);
+      R sc = (R)1;
+      if (lg >= (long double)kRescaleLog2) {
+        sc = (R)std::ldexp(1.0, -kRescaleLog2);
+        lg -= (long double)kRescaleLog2;
+      }
+      tans[(size_t)i * T + k] = tf;
+      scales[(size_t)i * T + k] = sc;
+      lg += 0.5L * (long double)geo[(size_t)i].n * std::log2(1.0L + (long double)tf * (long double)tf);
+    }
+  }
+
+  // phase tables per distinct n
+  std::map<int, std::vector<unsigned char>> tables;
+  std::map<int, typename PhaseV<R>::params> phase_of;
+  for (const Geo& g : geo) {
+    if (tables.count(g.n)) continue;
+    typename PhaseV<R>::params ph{};
+    std::vector<unsigned char> bytes;
+    if constexpr (sizeof(R) == 4) {
+      std::vector<float2> hab;
+      BK_TRY(build_phase_v(c, g.n, g.angle_unit, &ph, &hab));
+      bytes.resize(hab.size() * sizeof(float2));
+      std::memcpy(bytes.data(), hab.data(), bytes.size());
+    } else {
+      const int emax = (g.n - 1) * g.n * (2 * g.n - 1) / 6;
+      const int n_hi = (emax >> kPhaseLoBits) + 1;
+      std::vector<double2> t((size_t)n_hi + kPhaseLo);
+      for (int h = 0; h < n_hi; ++h) {
+        const double th = -g.angle_unit * (double)(h << kPhaseLoBits);
+        t[(size_t)h] = make_double2(std::cos(th), std::sin(th));
+      }
+      for (int l = 0; l < kPhaseLo; ++l) {
+        const double th = -g.angle_unit * (double)l;
+        t[(size_t)n_hi + l] = make_double2(std::cos(th), std::sin(th));
+      }
+      ph.n_hi = n_hi;
+      bytes.resize(t.size() * sizeof(double2));
+      std::memcpy(bytes.data(), t.data(), bytes.size());
+    }
+    tables[g.n] = std::move(bytes);
+    phase_of[g.n] = ph;
+  }
+
+  // tasks of one step: A1 blocks in order, each slab's S2 block `lag` blocks later, then S3
+  auto task = [](int kind, int in, uint32_t tile) {
+    return ((unsigned long long)kind << 56) | ((unsigned long long)in << 32) | tile;
+  };
+  std::vector<std::pair<int, uint32_t>> blocks;  // (instance, slab)
+  for (int i = 0; i < n_inst; ++i)
+    for (uint32_t h = 0; h < geo[(size_t)i].slabs; ++h) blocks.push_back({i, h});
+  const size_t lag = (size_t)std::max(1, bp->lag > 0 ? bp->lag : c->slab_lag);
+  std::vector<unsigned long long> tasks, final_tasks;
+  for (size_t j = 0; j < blocks.size() + lag; ++j) {
+    if (j < blocks.size()) {
+      const auto [i, h] = blocks[j];
+      const uint32_t per = 1u << geo[(size_t)i].w2;
+      for (uint32_t t = 0; t < per; ++t) tasks.push_back(task(TASK_A1, i, h * per + t));
+    }
+    if (j >= lag && j - lag < blocks.size()) {
+      const auto [i, h] = blocks[j - lag];
+      const uint32_t per = 1u << geo[(size_t)i].w2;
+      for (uint32_t t = 0; t < per; ++t) tasks.push_back(task(TASK_S2, i, h * per + t));
+    }
+  }
+  for (int i = 0; i < n_inst; ++i)
+    if (geo[(size_t)i].w3 > 0)
+      for (uint32_t t = 0; t < geo[(size_t)i].n_a1; ++t) tasks.push_back(task(TASK_S3, i, t));
+  if (slot[(size_t)T] >= 0)
+    for (int i = 0; i < n_inst; ++i)
+      for (uint32_t t = 0; t < geo[(size_t)i].n_a1; ++t) final_tasks.push_back(task(TASK_M, i, t));
+
+  // device buffer
+  Bump b;
+  const size_t o_maps = b.take((size_t)n_inst * 4 * sizeof(CUtensorMap));
+  const size_t o_desc = b.take((size_t)n_inst * sizeof(InstDesc<R>));
+  const size_t o_tasks = b.take(tasks.size() * 8);
+  const size_t o_final = b.take(std::max<size_t>(final_tasks.size(), 1) * 8);
+  const size_t o_tan = b.take(tans.size() * sizeof(R));
+  const size_t o_scale = b.take(scales.size() * sizeof(R));
+  const size_t o_slot = b.take(slot.size() * sizeof(int));
+  std::map<int, size_t> o_tab;
+  for (auto& kv : tables) o_tab[kv.first] = b.take(kv.second.size());
+  std::vector<size_t> o_ctr((size_t)n_inst), o_part((size_t)n_inst);
+  for (int i = 0; i < n_inst; ++i) {
+    o_ctr[(size_t)i] = b.take((geo[(size_t)i].slabs + 4) * sizeof(unsigned int));
+    o_part[(size_t)i] = b.take(3 * (size_t)geo[(size_t)i].n_a1 * sizeof(double));
+  }
+  const size_t o_glob = b.take(8 * sizeof(unsigned int));  // next, err, abort
+  const size_t o_offs = b.take((size_t)n_inst * sizeof(unsigned long long));
+  const size_t o_idx = b.take((size_t)n_inst * sizeof(unsigned int));
+  const size_t ctr_begin = o_ctr.empty() ? o_glob : o_ctr[0];
+  BK_TRY(ensure_buffer(c, &c->d_batch, &c->batch_cap, b.off));
+  char* base = static_cast<char*>(c->d_batch);
+  CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(base + o_maps);
+
+  std::vector<CUtensorMap> maps((size_t)n_inst * 4);
+  std::vector<InstDesc<R>> descs((size_t)n_inst);
+  std::vector<unsigned long long> offs((size_t)n_inst);
+  std::vector<unsigned int> idx((size_t)n_inst);
+  for (int i = 0; i < n_inst; ++i) {
+    const Geo& g = geo[(size_t)i];
+    uint16_t* dE = nullptr;
+    BK_TRY(batch_energy(c, g.n, &dE));
+    void* st = state + g.state_off;
+    TmaDesc a1m, em, m2, m3;
+    BK_TRY(build_amp_map(c, st, g.np, BK_C128, kElemBits, kElemBits, 0, &a1m));
+    BK_TRY(build_e_map(c, dE, g.n, c64 ? 13 : 12, &em));
+    BK_TRY(build_amp_map(c, st, g.np, BK_C128, kElemBits - g.w2, kElemBits, g.w2, &m2));
+    if (g.w3 > 0) BK_TRY(build_amp_map(c, st, g.np, BK_C128, kElemBits - g.w3, kElemBits + g.w2, g.w3, &m3));
+    maps[(size_t)i * 4 + 0] = a1m.map;
+    maps[(size_t)i * 4 + 1] = em.map;
+    maps[(size_t)i * 4 + 2] = m2.map;
+    maps[(size_t)i * 4 + 3] = g.w3 > 0 ? m3.map : m2.map;
+    InstDesc<R> D{};
+    D.state = static_cast<unsigned char*>(st);
+    D.map_a1 = d_maps + (size_t)i * 4 + 0;
+    D.map_e = d_maps + (size_t)i * 4 + 1;
+    D.map_s2 = d_maps + (size_t)i * 4 + 2;
+    D.map_s3 = d_maps + (size_t)i * 4 + 3;
+    D.np = g.np;
+    D.n = g.n;
+    D.w2 = g.w2;
+    D.w3 = g.w3;
+    D.a1_hi_dim = a1m.hi_dim;
+    D.s2_mid_dim = m2.mid_dim;
+    D.s2_hi_dim = m2.hi_dim;
+    D.s2_mid_bits = (int)m2.mid_bits;
+    D.s3_mid_dim = g.w3 > 0 ? m3.mid_dim : -1;
+    D.s3_hi_dim = g.w3 > 0 ? m3.hi_dim : -1;
+    D.s3_mid_bits = g.w3 > 0 ? (int)m3.mid_bits : 0;
+    D.e0 = g.e0;
+    D.s0 = g.s0;
+    typename PhaseV<R>::params ph = phase_of[g.n];
+    if constexpr (sizeof(R) == 4) {
+      ph.hab = reinterpret_cast<const float2*>(base + o_tab[g.n]);
+    } else {
+      ph.hi = reinterpret_cast<const double2*>(base + o_tab[g.n]);
+      ph.lo = ph.hi + ph.n_hi;
+    }
+    D.phase = ph;
+    D.tan = reinterpret_cast<const R*>(base + o_tan) + (size_t)i * T;
+    D.scale = reinterpret_cast<const R*>(base + o_scale) + (size_t)i * T;
+    D.slot = reinterpret_cast<const int*>(base + o_slot);
+    unsigned int* ctr = reinterpret_cast<unsigned int*>(base + o_ctr[(size_t)i]);
+    D.a1_done = ctr;
+    D.s2_done = ctr + g.slabs;
+    D.s3_done = ctr + g.slabs + 1;
+    D.ticket = ctr + g.slabs + 2;
+    D.partials = reinterpret_cast<double*>(base + o_part[(size_t)i]);
+    D.results = c->d_batch_results + (size_t)i * n_meas * 4;
+    D.n_a1 = g.n_a1;
+    D.n_s2 = g.n_a1;
+    D.n_s3 = g.w3 > 0 ? g.n_a1 : 0u;
+    D.inverse = 0;
+    descs[(size_t)i] = D;
+    offs[(size_t)i] = g.state_off;
+    idx[(size_t)i] = g.s0;
+  }
+  cudaStream_t st = c->stream;
+  BK_CUDA(c, cudaMemcpyAsync(d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemcpyAsync(base + o_desc, descs.data(), descs.size() * sizeof(InstDesc<R>), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemcpyAsync(base + o_tasks, tasks.data(), tasks.size() * 8, cudaMemcpyHostToDevice, st));
+  if (!final_tasks.empty())
+    BK_CUDA(c, cudaMemcpyAsync(base + o_final, final_tasks.data(), final_tasks.size() * 8, cudaMemcpyHostToDevice, st));
+  if (T > 0) {
+    BK_CUDA(c, cudaMemcpyAsync(base + o_tan, tans.data(), tans.size() * sizeof(R), cudaMemcpyHostToDevice, st));
+    BK_CUDA(c, cudaMemcpyAsync(base + o_scale, scales.data(), scales.size() * sizeof(R), cudaMemcpyHostToDevice, st));
+  }
+  BK_CUDA(c, cudaMemcpyAsync(base + o_slot, slot.data(), slot.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  for (auto& kv : tables)
+    BK_CUDA(c, cudaMemcpyAsync(base + o_tab[kv.first], kv.second.data(), kv.second.size(), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemcpyAsync(base + o_offs, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemcpyAsync(base + o_idx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, st));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R>), PersistSmem::kBytes));
+
+  Program P{};
+  P.tasks = reinterpret_cast<const unsigned long long*>(base + o_tasks);
+  P.per_step = (uint32_t)tasks.size();
+  P.n_steps = (uint32_t)T;
+  P.final_tasks = reinterpret_cast<const unsigned long long*>(base + o_final);
+  P.n_final = (uint32_t)final_tasks.size();
+  P.step0 = 0;
+  unsigned int* glob = reinterpret_cast<unsigned int*>(base + o_glob);
+  P.next = glob;
+  P.err = reinterpret_cast<int*>(glob + 1);
+  P.abort = reinterpret_cast<int*>(glob + 2);
+  const InstDesc<R>* dd = reinterpret_cast<const InstDesc<R>*>(base + o_desc);
+
+  // the whole run: zero the states and counters, set the basis states, one persistent launch
+  auto enqueue = [&]() -> int {
+    BK_CUDA(c, cudaMemsetAsync(state, 0, state_bytes, st));
+    BK_CUDA(c, cudaMemsetAsync(base + ctr_begin, 0, o_glob + 8 * sizeof(unsigned int) - ctr_begin, st));
+    set_basis_many_kernel<<<(n_inst + 127) / 128, 128, 0, st>>>(state, reinterpret_cast<unsigned long long*>(base + o_offs),
+                                                                reinterpret_cast<unsigned int*>(base + o_idx),
+                                                                c64 ? 1 : 0, n_inst);
+    BK_CUDA(c, cudaGetLastError());
+    persist_kernel<R><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(dd, P);
+    BK_CUDA(c, cudaGetLastError());
+    return BK_OK;
+  };
+  size_t ev = 0;
+  BK_TRY(ev_begin(c, "batch", &ev));
+  if (bp->use_graph) {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    BK_CUDA(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int r = enqueue();
+    cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (r != BK_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return r;
+    }
+    BK_CUDA(c, ce);
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    BK_CUDA(c, ce);
+    ce = cudaGraphLaunch(exec, st);
+    cudaGraphExecDestroy(exec);  // destruction is deferred until the launch completes
+    BK_CUDA(c, ce);
+  } else {
+    BK_TRY(enqueue());
+  }
+  BK_TRY(ev_end(c, ev));
+  std::vector<double> rows((size_t)n_inst * n_meas * 4);
+  int e = 0;
+  BK_CUDA(c, cudaMemcpyAsync(&e, P.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (!rows.empty())
+    BK_CUDA(c, cudaMemcpyAsync(rows.data(), c->d_batch_results, rows.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  BK_CUDA(c, cudaStreamSynchronize(st));
+  BK_TRY(collect_timing(c));
+  if (e != 0) return fail(c, BK_ERR_TIMEOUT, "batched persistent engine: a bounded device wait gave up (%d)", e);
+  for (int i = 0; i < n_inst; ++i)
+    for (int m = 0; m < n_meas; ++m) {
+      const size_t r = (size_t)i * n_meas + m;
+      const long double f = std::exp2(-2.0L * row_log2[r]);
+      p_less[r] = (double)((long double)rows[4 * r + 0] * f);
+      d_h[r] = (double)((long double)rows[4 * r + 1] * f);
+      if (norm_out) norm_out[r] = (double)((long double)rows[4 * r + 2] * f);
+    }
   return BK_OK;
 }
 
@@ -872,68 +1322,6 @@ int check_device_error(bk_ctx* c) {
 
 }  // namespace
 
-// ---- trap generation (host) ----
-static int64_t host_energy(int n, uint64_t x) {
-  int64_t e = 0;
-  for (int k = 1; k < n; ++k) {
-    const int64_t ck = (int64_t)(n - k) - 2 * (int64_t)__builtin_popcountll((x ^ (x >> k)) & ((1ull << (n - k)) - 1ull));
-    e += ck * ck;
-  }
-  return e;
-}
-
-// Optimal LABS energies E*(n) for n <= 32 (reference: labs_energy.hpp:156-168).
-static int64_t optimal_energy(int n) {
-  static const int64_t t[33] = {-1, -1, -1, 1, 2, 2, 7, 3, 8, 12, 13, 5, 10, 6, 19, 15, 24,
-                                32, 25, 29, 26, 26, 39, 47, 36, 36, 45, 37, 50, 62, 59, 67, 64};
-  return (n >= 0 && n <= 32) ? t[n] : -1;
-}
-
-// One descent with incremental C_k (reference: classical.cuh:625-712). Each
-// sweep costs n evaluations; a flip is taken only when strictly better, the
-// lowest bit index winning ties.
-static void descend(int n, uint64_t start, uint64_t max_evals, uint64_t* fs, int64_t* fe, uint64_t* ev) {
-  const uint64_t budget = max_evals == 0 ? ~0ull : max_evals;
-  uint64_t x = start;
-  int64_t C[64];
-  int64_t e = 0;
-  for (int k = 1; k < n; ++k) {
-    C[k] = (int64_t)(n - k) - 2 * (int64_t)__builtin_popcountll((x ^ (x >> k)) & ((1ull << (n - k)) - 1ull));
-    e += C[k] * C[k];
-  }
-  uint64_t evals = 1;
-  while (evals + (uint64_t)n <= budget) {
-    int best = -1;
-    int64_t best_e = e;
-    for (int p = 0; p < n; ++p) {
-      const int sp = ((x >> p) & 1ull) ? -1 : 1;
-      int64_t ne = 0;
-      for (int k = 1; k < n; ++k) {
-        int64_t d = 0;
-        if (p + k < n) d -= 2 * sp * (((x >> (p + k)) & 1ull) ? -1 : 1);
-        if (p - k >= 0) d -= 2 * sp * (((x >> (p - k)) & 1ull) ? -1 : 1);
-        ne += (C[k] + d) * (C[k] + d);
-      }
-      if (ne < best_e) {
-        best_e = ne;
-        best = p;
-      }
-    }
-    evals += (uint64_t)n;
-    if (best < 0) break;
-    const int sp = ((x >> best) & 1ull) ? -1 : 1;
-    for (int k = 1; k < n; ++k) {
-      if (best + k < n) C[k] -= 2 * sp * (((x >> (best + k)) & 1ull) ? -1 : 1);
-      if (best - k >= 0) C[k] -= 2 * sp * (((x >> (best - k)) & 1ull) ? -1 : 1);
-    }
-    x ^= 1ull << best;
-    e = best_e;
-  }
-  *fs = x;
-  *fe = e;
-  if (ev) *ev = evals;
-}
-
 // ============================================================================
 // C ABI
 // ============================================================================
@@ -991,6 +1379,9 @@ int bk_destroy(bk_ctx* c) {
   for (void* p : {(void*)c->d_E, c->d_state, (void*)c->d_partials, (void*)c->d_results, (void*)c->d_ticket,
                   (void*)c->d_err, (void*)c->d_count, c->d_phase, c->d_small, (void*)c->d_chunks, c->d_io,
                   (void*)c->d_rand, (void*)c->d_samples, (void*)c->d_binom, (void*)c->d_found})
+    if (p) cudaFree(p);
+  for (auto& kv : c->batch_E) cudaFree(kv.second);
+  for (void* p : {c->d_batch_state, c->d_batch, (void*)c->d_batch_results, c->d_persist})
     if (p) cudaFree(p);
   for (auto& e : c->ev_pool) {
     cudaEventDestroy(e.first);
@@ -1076,6 +1467,31 @@ int bk_p_blind(bk_ctx* c, int n, int64_t e0, uint64_t* count_out, double* p_out)
   if (count_out) *count_out = h;
   if (p_out) *p_out = (double)h / (double)count;
   return BK_OK;
+}
+
+int bk_set_option(bk_ctx* c, int option, int64_t value) {
+  if (!c) return BK_ERR_INVALID;
+  switch (option) {
+    case BK_OPT_ENGINE_MODE:
+      if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "engine mode %lld", (long long)value);
+      c->engine_mode = (int)value;
+      return BK_OK;
+    case BK_OPT_SLAB_LAG:
+      if (value < 1 || value > 64) return fail(c, BK_ERR_INVALID, "slab lag %lld", (long long)value);
+      c->slab_lag = (int)value;
+      return BK_OK;
+    default:
+      return fail(c, BK_ERR_INVALID, "unknown option %d", option);
+  }
+}
+
+int bk_get_option(const bk_ctx* c, int option, int64_t* value) {
+  if (!c || !value) return BK_ERR_INVALID;
+  switch (option) {
+    case BK_OPT_ENGINE_MODE: *value = c->engine_mode; return BK_OK;
+    case BK_OPT_SLAB_LAG: *value = c->slab_lag; return BK_OK;
+    default: return BK_ERR_INVALID;
+  }
 }
 
 int bk_stream(bk_ctx* c, void** out) {
@@ -1498,6 +1914,19 @@ int bk_sampler_run(bk_ctx* c, const bk_sampler_config* cfg, uint64_t start_bits,
               << std::setprecision(4) << out->per_eval_rate << std::defaultfloat << "\n";
   }
   return BK_OK;
+}
+
+int bk_evolve_batch(bk_ctx* c, const bk_batch_params* p, const bk_batch_instance* inst, int32_t n_inst,
+                    double* p_less, double* d_h, double* norm) {
+  if (!c || !p || (n_inst > 0 && !inst) || n_inst < 0) return BK_ERR_INVALID;
+  if (n_inst == 0) return BK_OK;
+  if (n_inst > (1 << 16)) return fail(c, BK_ERR_UNSUPPORTED, "at most 65536 instances per batch");
+  if (p->n_steps < 0 || !is_finite(p->dt) || !is_finite(p->diag_scale))
+    return fail(c, BK_ERR_INVALID, "invalid batch parameters");
+  if (p->precision != BK_C64 && p->precision != BK_C128) return fail(c, BK_ERR_INVALID, "precision %d", p->precision);
+  BK_CUDA(c, cudaSetDevice(c->device));
+  if (p->precision == BK_C64) return evolve_batch_t<float>(c, p, inst, n_inst, p_less, d_h, norm);
+  return evolve_batch_t<double>(c, p, inst, n_inst, p_less, d_h, norm);
 }
 
 int bk_export_state(bk_ctx* c, double* host) {

@@ -22,12 +22,14 @@
 // written by A1 is re-read by S2 while it is still in L2: A1 + S2 together cost
 // one HBM round trip.
 //
-// CTA = 8 compute warps + 1 producer warp. The producer claims tasks from a
-// global counter (in order, so every dependency points to an earlier task held
-// by a running CTA: no deadlock), waits (bounded) for the dependency, and TMA-
-// loads the tile into one of two shared-memory stages; the compute warps work
-// on the other stage. All waits are bounded and a global abort word stops every
-// CTA after the first failure.
+// Two CTAs per SM (256 threads, one 80 KB stage each), so one CTA's stores and
+// completion fence overlap the other's arithmetic. Thread 0 claims tasks from a
+// global counter in order (every dependency points to an earlier task held by a
+// running CTA, and a CTA signals its finished task before it waits on the next
+// one's dependency: no deadlock), waits (bounded) for the dependency and issues
+// the TMA; when the next task's dependency is already met its load is issued
+// while the current task's stores drain. All waits are bounded and a global
+// abort word stops every CTA after the first failure.
 #pragma once
 #include "bk_device.cuh"
 #include "bk_fused.cuh"
@@ -37,9 +39,8 @@ namespace bk {
 constexpr int kElemBits = 12;          // 4096 elements per tile
 constexpr int kStageTileBytes = 65536;
 constexpr int kStageEBytes = 16384;    // A1: uint16 E of 8192 (c64) / 4096 (c128) amplitudes
-constexpr int kStages = 2;
 constexpr int kComputeThreads = 256;
-constexpr int kPersistThreads = kComputeThreads + 32;
+constexpr int kPersistThreads = kComputeThreads;
 
 enum TaskKind : int { TASK_A1 = 0, TASK_S2 = 1, TASK_S3 = 2, TASK_M = 3, TASK_END = 7 };
 
@@ -61,6 +62,9 @@ struct El<float> {
   }
   __device__ static void st(void* p, const T& v) {
     *reinterpret_cast<float4*>(p) = make_float4(v.re.x, v.re.y, v.im.x, v.im.y);
+  }
+  __device__ static void stg(void* p, const T& v, uint64_t pol) {
+    st_global_hint(p, make_float4(v.re.x, v.re.y, v.im.x, v.im.y), pol);
   }
   // a' = a + i t b, b' = b + i t a on both amplitudes of the elements at once
   __device__ static void bfly(T& a, T& b, float t) {
@@ -108,6 +112,7 @@ struct El<double> {
   static constexpr int kAmps = 1;
   __device__ static T ld(const void* p) { return T{*reinterpret_cast<const double2*>(p)}; }
   __device__ static void st(void* p, const T& v) { *reinterpret_cast<double2*>(p) = v.v; }
+  __device__ static void stg(void* p, const T& v, uint64_t pol) { st_global_hint(p, v.v, pol); }
   __device__ static void bfly(T& a, T& b, double t) { bk::bfly(a.v, b.v, t); }
   __device__ static void bfly_inner(T&, double) {}
   __device__ static T shfl_xor(const T& v, int m) {
@@ -272,9 +277,7 @@ __device__ __forceinline__ void fence_proxy_async_global() {
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
-__device__ __forceinline__ void compute_sync() {
-  asm volatile("bar.sync 1, %0;" ::"n"(kComputeThreads) : "memory");
-}
+__device__ __forceinline__ void compute_sync() { __syncthreads(); }
 __device__ __forceinline__ bool aborted(const int* abort) {
   return *reinterpret_cast<const volatile int*>(abort) != 0;
 }
@@ -328,11 +331,11 @@ __device__ __forceinline__ void el_bflys(typename El<R>::T (&v)[16], R t) {
 }
 template <class R, uint32_t REG, int CP>
 __device__ __forceinline__ void el_gstore(unsigned char* g, const typename El<R>::T (&v)[16], uint32_t tile_base,
-                                          uint32_t base, uint32_t h0) {
+                                          uint32_t base, uint32_t h0, uint64_t pol) {
   const uint32_t gb = tile_base | tile_to_global<CP>(base, h0);
 #pragma unroll
   for (int j = 0; j < 16; ++j)
-    El<R>::st(g + 16ull * (gb | tile_to_global<CP>(pdep((uint32_t)j, REG), h0)), v[j]);
+    El<R>::stg(g + 16ull * (gb | tile_to_global<CP>(pdep((uint32_t)j, REG), h0)), v[j], pol);
 }
 
 // measurement helpers on an element with E (c64: two uint16 packed)
@@ -414,10 +417,13 @@ __device__ __forceinline__ void compute_reduce(MeasureAcc acc, double* partials,
 }
 
 // A1 (and measurement-only M) on a staged tile
-template <class R, bool MEASURE_ONLY>
+// `stage_free()` runs (in every thread, after a barrier) as soon as the last
+// shared-memory read of the staged tile is done, so the next tile's load can be
+// issued while this tile's last round computes and its stores drain.
+template <class R, bool MEASURE_ONLY, class F>
 __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned char* etile, const InstDesc<R>& D,
                                            uint32_t t_idx, uint32_t step, const unsigned char* phase_smem,
-                                           double* red, int* last_flag) {
+                                           double* red, int* last_flag, F&& stage_free) {
   using PL = Plan<double>;
   using E = El<R>;
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -428,11 +434,21 @@ __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned c
   const int slot = D.slot[step];
   MeasureAcc acc;
   const R t = MEASURE_ONLY ? (R)0 : D.tan[step];
+  if (MEASURE_ONLY) {
+    // measurement only: read the E values first, then release the stage
+    uint32_t ev[16];
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
+    for (int j = 0; j < 16; ++j) ev[j] = load_e<R>(etile, b1 | pdep((uint32_t)j, PL::A1_R1_REG));
+    __syncthreads();
+    stage_free();
+#pragma unroll
+    for (int j = 0; j < 16; ++j) measure_el(acc, v[j], ev[j], tile_base | (b1 | pdep((uint32_t)j, PL::A1_R1_REG)), D.e0, D.s0);
+  }
+#pragma unroll
+  for (int j = 0; j < 16 && !MEASURE_ONLY; ++j) {
     const uint32_t i = b1 | pdep((uint32_t)j, PL::A1_R1_REG);
     const uint32_t e = load_e<R>(etile, i);
-    if (MEASURE_ONLY || slot >= 0) measure_el(acc, v[j], e, tile_base | i, D.e0, D.s0);
+    if (slot >= 0) measure_el(acc, v[j], e, tile_base | i, D.e0, D.s0);
     if (!MEASURE_ONLY) {
       PhaseV<R>::apply(v[j], e, D.phase, phase_smem, false);
       E::bfly_inner(v[j], t);
@@ -456,8 +472,10 @@ __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned c
     compute_sync();
     const uint32_t b3 = pdep(lane, PL::A1_R3_LANE) | pdep(warp, PL::A1_R3_WARP);
     el_load<R, PL::A1_R3_REG, true>(tile, v, b3);
+    __syncthreads();
+    stage_free();
     el_bflys<R, PL::A1_R3_REG, PL::A1_R3_ACT>(v, t);
-    el_gstore<R, PL::A1_R3_REG, kElemBits>(D.state, v, tile_base, b3, 0);
+    el_gstore<R, PL::A1_R3_REG, kElemBits>(D.state, v, tile_base, b3, 0, policy_evict_last());
   }
   if (MEASURE_ONLY || slot >= 0)
     compute_reduce(acc, D.partials, D.ticket, D.results, MEASURE_ONLY ? D.slot[step] : slot, t_idx, D.n_a1, red,
@@ -465,9 +483,9 @@ __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned c
 }
 
 // strided pass of width W on a staged tile (element bits [0, 12 - W) u [h0, h0 + W))
-template <class R, int W>
+template <class R, int W, class F>
 __device__ __forceinline__ void process_s(unsigned char* tile, unsigned char* state, uint32_t tile_base,
-                                          uint32_t h0, R t) {
+                                          uint32_t h0, R t, F&& stage_free) {
   using PL = Plan<double>;
   using E = El<R>;
   constexpr int CP = kElemBits - W;
@@ -476,9 +494,13 @@ __device__ __forceinline__ void process_s(unsigned char* tile, unsigned char* st
   constexpr uint32_t ACT_ALL = ((1u << W) - 1u) << CP;
   const uint32_t b1 = pdep(lane, PL::S_R1_LANE) | pdep(warp, PL::S_R1_WARP);
   el_load<R, PL::S_R1_REG, false>(tile, v, b1);
+  if constexpr (W <= 4) {
+    __syncthreads();
+    stage_free();
+  }
   el_bflys<R, PL::S_R1_REG, ACT_ALL>(v, t);
   if constexpr (W <= 4) {
-    el_gstore<R, PL::S_R1_REG, CP>(state, v, tile_base, b1, h0);
+    el_gstore<R, PL::S_R1_REG, CP>(state, v, tile_base, b1, h0, policy_evict_first());
   } else {
     using R2 = StridedR2<double, W>;
     compute_sync();
@@ -486,6 +508,8 @@ __device__ __forceinline__ void process_s(unsigned char* tile, unsigned char* st
     compute_sync();
     const uint32_t b2 = pdep(lane, R2::LANE) | pdep(warp, R2::WARP);
     el_load<R, R2::REG, true>(tile, v, b2);
+    __syncthreads();
+    stage_free();
     el_bflys<R, R2::REG, R2::ACT>(v, t);
     if constexpr (R2::kShuffleLaneBit >= 0) {
 #pragma unroll
@@ -494,183 +518,200 @@ __device__ __forceinline__ void process_s(unsigned char* tile, unsigned char* st
         E::bfly_partner(v[j], q, t);
       }
     }
-    el_gstore<R, R2::REG, CP>(state, v, tile_base, b2, h0);
+    el_gstore<R, R2::REG, CP>(state, v, tile_base, b2, h0, policy_evict_first());
   }
 }
 
-template <class R>
+template <class R, class F>
 __device__ __forceinline__ void process_s_dispatch(int w, unsigned char* tile, unsigned char* state,
-                                                   uint32_t tile_base, uint32_t h0, R t) {
+                                                   uint32_t tile_base, uint32_t h0, R t, F&& f) {
   switch (w) {
-    case 1: process_s<R, 1>(tile, state, tile_base, h0, t); break;
-    case 2: process_s<R, 2>(tile, state, tile_base, h0, t); break;
-    case 3: process_s<R, 3>(tile, state, tile_base, h0, t); break;
-    case 4: process_s<R, 4>(tile, state, tile_base, h0, t); break;
-    case 5: process_s<R, 5>(tile, state, tile_base, h0, t); break;
-    case 6: process_s<R, 6>(tile, state, tile_base, h0, t); break;
-    case 7: process_s<R, 7>(tile, state, tile_base, h0, t); break;
-    case 8: process_s<R, 8>(tile, state, tile_base, h0, t); break;
-    default: process_s<R, 9>(tile, state, tile_base, h0, t); break;
+    case 1: process_s<R, 1>(tile, state, tile_base, h0, t, f); break;
+    case 2: process_s<R, 2>(tile, state, tile_base, h0, t, f); break;
+    case 3: process_s<R, 3>(tile, state, tile_base, h0, t, f); break;
+    case 4: process_s<R, 4>(tile, state, tile_base, h0, t, f); break;
+    case 5: process_s<R, 5>(tile, state, tile_base, h0, t, f); break;
+    case 6: process_s<R, 6>(tile, state, tile_base, h0, t, f); break;
+    case 7: process_s<R, 7>(tile, state, tile_base, h0, t, f); break;
+    case 8: process_s<R, 8>(tile, state, tile_base, h0, t, f); break;
+    default: process_s<R, 9>(tile, state, tile_base, h0, t, f); break;
   }
 }
 
 // ---------------------------------------------------------------------------
-// the persistent kernel
+// the persistent kernel: 2 CTAs per SM, one stage each; thread 0 claims tasks,
+// waits (bounded) for their dependencies and issues the TMA; the next task's
+// load is issued early, while this task's stores drain, whenever its
+// dependency is already met (never blocking before this task has signalled).
 // ---------------------------------------------------------------------------
 struct PersistSmem {
   static constexpr int kStageBytes = kStageTileBytes + kStageEBytes;
-  static constexpr int kMetaOff = kStages * kStageBytes;
-  static constexpr int kPhaseOff = kMetaOff + 256;
+  static constexpr int kPhaseOff = kStageBytes;
   static constexpr int kRedOff = kPhaseOff + 3328;  // >= both phase table footprints
   static constexpr int kBytes = kRedOff + 256;
 };
 
 template <class R>
-__global__ void __launch_bounds__(kPersistThreads, 1)
+__device__ __forceinline__ bool decode_task(const Program& P, uint32_t g, StageMeta& m) {
+  if (g >= P.per_step * P.n_steps + P.n_final) return false;
+  unsigned long long task;
+  uint32_t k;
+  if (g < P.per_step * P.n_steps) {
+    k = g / P.per_step;
+    task = P.tasks[g - k * P.per_step];
+  } else {
+    k = P.n_steps;
+    task = P.final_tasks[g - P.per_step * P.n_steps];
+  }
+  m.kind = (int)(task >> 56);
+  m.inst = (int)((task >> 32) & 0xFFFFFFu);
+  m.tile = (uint32_t)task;
+  m.step = k;
+  return true;
+}
+
+// dependency of a task: counter and target (ctr == nullptr: none)
+template <class R>
+__device__ __forceinline__ const unsigned int* task_dep(const InstDesc<R>& D, const StageMeta& m, uint32_t& target) {
+  if (m.kind == TASK_A1 || m.kind == TASK_M) {
+    if (m.step == 0) return nullptr;
+    target = (D.w3 > 0 ? D.n_s3 : D.n_s2) * m.step;
+    return D.w3 > 0 ? D.s3_done : D.s2_done;
+  }
+  if (m.kind == TASK_S2) {
+    target = (1u << D.w2) * (m.step + 1u);
+    return D.a1_done + (m.tile >> D.w2);
+  }
+  target = D.n_s2 * (m.step + 1u);
+  return D.s2_done;
+}
+
+template <class R>
+__device__ __forceinline__ void issue_task_load(const InstDesc<R>& D, const StageMeta& m, unsigned char* stage,
+                                                uint32_t fb) {
+  if (m.kind == TASK_A1 || m.kind == TASK_M) {
+    mbar_arrive_expect_tx(fb, (uint32_t)(kStageTileBytes + 4096 * 2 * El<R>::kAmps));
+    const int hd = D.a1_hi_dim;
+    const uint64_t pol = policy_evict_first();
+    tma_load_5d_hint(smem_addr(stage), D.map_a1, 0, 0, hd == 2 ? (int)m.tile : 0, hd == 3 ? (int)m.tile : 0, 0, fb,
+                     pol);
+    tma_load_5d_hint(smem_addr(stage + kStageTileBytes), D.map_e, 0, 0, (int)m.tile, 0, 0, fb, pol);
+  } else {
+    const bool s2 = (m.kind == TASK_S2);
+    const int mb = s2 ? D.s2_mid_bits : D.s3_mid_bits;
+    const int md = s2 ? D.s2_mid_dim : D.s3_mid_dim;
+    const int hd = s2 ? D.s2_hi_dim : D.s3_hi_dim;
+    const int mid = (int)(m.tile & ((1u << mb) - 1u)), hi = (int)(m.tile >> mb);
+    mbar_arrive_expect_tx(fb, (uint32_t)kStageTileBytes);
+    tma_load_5d_hint(smem_addr(stage), s2 ? D.map_s2 : D.map_s3, tile_coord(0, md, mid, hd, hi),
+                     tile_coord(1, md, mid, hd, hi), tile_coord(2, md, mid, hd, hi), tile_coord(3, md, mid, hd, hi),
+                     tile_coord(4, md, mid, hd, hi), fb, policy_evict_first());
+  }
+}
+
+// bounded wait for a dependency counter (thread 0); false on timeout / abort
+__device__ __forceinline__ bool wait_counter(const unsigned int* ctr, uint32_t target, const Program& P) {
+  uint32_t polls = 0;
+  while (ld_acquire(ctr) < target) {
+    if (++polls > kWaitPolls * 4u) {
+      raise_error(P, DEV_TIMEOUT);
+      return false;
+    }
+    if ((polls & 63u) == 0u && aborted(P.abort)) return false;
+    __nanosleep(32);
+  }
+  fence_proxy_async_global();  // the TMA (async proxy) must see the data the counter released
+  return true;
+}
+
+template <class R>
+__device__ __forceinline__ bool dep_met(const unsigned int* ctr, uint32_t target, uint32_t seen) {
+  return ctr == nullptr || seen >= target;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kComputeThreads, 2)
     persist_kernel(const InstDesc<R>* __restrict__ insts, const Program P) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
+  __shared__ __align__(8) uint64_t full_bar;
   __shared__ int last_flag;
   __shared__ int cur_phase_inst;
-  StageMeta* meta = reinterpret_cast<StageMeta*>(smem + PersistSmem::kMetaOff);
+  __shared__ StageMeta cur, nxt;
+  __shared__ uint32_t g_after;
+  __shared__ int inflight;  // a tile load is issued and not yet consumed
+  __shared__ int early;     // the current task's stage_free() issued the next load
+  unsigned char* stage = smem;
   unsigned char* phase_smem = smem + PersistSmem::kPhaseOff;
   double* red = reinterpret_cast<double*>(smem + PersistSmem::kRedOff);
   const int tid = threadIdx.x;
+  const uint32_t fb = smem_addr(&full_bar);
+  // thread 0 keeps the next task decoded (nxt) and the one after that claimed
+  // (g_after), so the claim's atomic and the dependency load are in flight while
+  // the tile computes
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(smem_addr(&full_bar[s]), 1);
-      mbar_init(smem_addr(&empty_bar[s]), 1);
-    }
+    mbar_init(fb, 1);
     fence_barrier_init();
     cur_phase_inst = -1;
+    inflight = 0;
+    const uint32_t g0 = atomicAdd(P.next, 1u);
+    const uint32_t g1 = atomicAdd(P.next, 1u);
+    if (!decode_task<R>(P, g0, cur)) {
+      cur.kind = TASK_END;
+    } else {
+      const InstDesc<R>& D = insts[cur.inst];
+      uint32_t target = 0;
+      const unsigned int* ctr = task_dep(D, cur, target);
+      if (ctr && !wait_counter(ctr, target, P)) cur.kind = TASK_END;
+      if (cur.kind != TASK_END) {
+        issue_task_load(D, cur, stage, fb);
+        inflight = 1;
+      }
+    }
+    if (!decode_task<R>(P, g1, nxt)) nxt.kind = TASK_END;
+    g_after = 0xFFFFFFFFu;
   }
   __syncthreads();
-
-  const uint32_t total = P.per_step * P.n_steps + P.n_final;
-
-  if (tid >= kComputeThreads) {
-    // ------------------------------ producer ------------------------------
-    if (tid != kComputeThreads) return;
-    uint32_t use[kStages] = {0, 0};
-    int s = 0;
-    bool stop = false;
-    while (!stop) {
-      const uint32_t g = aborted(P.abort) ? total : atomicAdd(P.next, 1u);
-      StageMeta m;
-      uint32_t bytes = 0;
-      if (g >= total) {
-        m.kind = TASK_END;
-        stop = true;
-      } else {
-        unsigned long long task;
-        uint32_t k;
-        if (g < P.per_step * P.n_steps) {
-          k = g / P.per_step;
-          task = P.tasks[g - k * P.per_step];
-        } else {
-          k = P.n_steps;
-          task = P.final_tasks[g - P.per_step * P.n_steps];
-        }
-        m.kind = (int)(task >> 56);
-        m.inst = (int)((task >> 32) & 0xFFFFFFu);
-        m.tile = (uint32_t)task;
-        m.step = k;  // step index inside this launch
-      }
-      // wait for the stage to be free
-      if (use[s] > 0 && !mbar_wait_or_abort(smem_addr(&empty_bar[s]), (use[s] - 1u) & 1u, P)) {
-        m.kind = TASK_END;
-        stop = true;
-      }
-      if (m.kind != TASK_END) {
-        const InstDesc<R>& D = insts[m.inst];
-        // dependency
-        const unsigned int* ctr = nullptr;
-        uint32_t target = 0;
-        const uint32_t kk = m.step;
-        if (m.kind == TASK_A1 || m.kind == TASK_M) {
-          if (kk > 0) {
-            ctr = D.w3 > 0 ? D.s3_done : D.s2_done;
-            target = (D.w3 > 0 ? D.n_s3 : D.n_s2) * kk;
-          }
-        } else if (m.kind == TASK_S2) {
-          ctr = D.a1_done + (m.tile >> D.w2);
-          target = (1u << D.w2) * (kk + 1u);
-        } else {
-          ctr = D.s2_done;
-          target = D.n_s2 * (kk + 1u);
-        }
-        if (ctr) {
-          uint32_t polls = 0;
-          while (ld_acquire(ctr) < target) {
-            if (++polls > kWaitPolls * 4u) {
-              raise_error(P, DEV_TIMEOUT);
-              break;
-            }
-            if ((polls & 63u) == 0u && aborted(P.abort)) break;
-            __nanosleep(64);
-          }
-          if (aborted(P.abort)) {
-            m.kind = TASK_END;
-            stop = true;
-          }
-          fence_proxy_async_global();
-        }
-        if (m.kind != TASK_END) {
-          const uint32_t fb = smem_addr(&full_bar[s]);
-          unsigned char* dst = smem + s * PersistSmem::kStageBytes;
-          meta[s] = m;
-          if (m.kind == TASK_A1 || m.kind == TASK_M) {
-            bytes = kStageTileBytes + (uint32_t)(4096 * 2 * El<R>::kAmps);
-            mbar_arrive_expect_tx(fb, bytes);
-            const int hd = D.a1_hi_dim;
-            tma_load_5d(smem_addr(dst), D.map_a1, 0, 0, hd == 2 ? (int)m.tile : 0, hd == 3 ? (int)m.tile : 0, 0, fb);
-            tma_load_5d(smem_addr(dst + kStageTileBytes), D.map_e, 0, 0, (int)m.tile, 0, 0, fb);
-          } else {
-            const bool s2 = (m.kind == TASK_S2);
-            const int mb = s2 ? D.s2_mid_bits : D.s3_mid_bits;
-            const int md = s2 ? D.s2_mid_dim : D.s3_mid_dim;
-            const int hd = s2 ? D.s2_hi_dim : D.s3_hi_dim;
-            const int mid = (int)(m.tile & ((1u << mb) - 1u)), hi = (int)(m.tile >> mb);
-            bytes = kStageTileBytes;
-            mbar_arrive_expect_tx(fb, bytes);
-            tma_load_5d(smem_addr(dst), s2 ? D.map_s2 : D.map_s3, tile_coord(0, md, mid, hd, hi),
-                        tile_coord(1, md, mid, hd, hi), tile_coord(2, md, mid, hd, hi),
-                        tile_coord(3, md, mid, hd, hi), tile_coord(4, md, mid, hd, hi), fb);
-          }
-        }
-      }
-      if (m.kind == TASK_END) {
-        meta[s] = m;
-        mbar_arrive(smem_addr(&full_bar[s]));
-      }
-      ++use[s];
-      s ^= 1;
-    }
-    // let in-flight loads land before leaving (bounded)
-    for (int q = 0; q < kStages; ++q)
-      if (use[q] > 0) mbar_wait_bounded(smem_addr(&full_bar[q]), (use[q] - 1u) & 1u, P.err);
-    return;
-  }
-
-  // ------------------------------ consumers ------------------------------
-  int s = 0;
-  uint32_t use[kStages] = {0, 0};
+  uint32_t phase = 0;
   for (;;) {
-    if (!mbar_wait_or_abort(smem_addr(&full_bar[s]), use[s] & 1u, P)) break;
-    const StageMeta m = meta[s];
+    const StageMeta m = cur;
     if (m.kind == TASK_END) break;
+    // thread 0: claim the task after next, read the next task's dependency early
+    const unsigned int* nctr = nullptr;
+    uint32_t ntarget = 0, nseen = 0;
+    if (tid == 0) {
+      g_after = aborted(P.abort) ? 0xFFFFFFFFu : atomicAdd(P.next, 1u);
+      if (nxt.kind != TASK_END) {
+        nctr = task_dep(insts[nxt.inst], nxt, ntarget);
+        if (nctr) nseen = ld_acquire(nctr);
+      }
+    }
+    if (!mbar_wait_or_abort(fb, phase, P)) break;
+    phase ^= 1u;
+    if (tid == 0) inflight = 0;
     const InstDesc<R>& D = insts[m.inst];
-    unsigned char* tile = smem + s * PersistSmem::kStageBytes;
+    // stage free: issue the next task's load now if its dependency is met
+    auto stage_free = [&]() {
+      if (tid == 0) {
+        early = 0;
+        if (nxt.kind != TASK_END && dep_met<R>(nctr, ntarget, nseen)) {
+          if (nctr) fence_proxy_async_global();
+          issue_task_load(insts[nxt.inst], nxt, stage, fb);
+          inflight = 1;
+          early = 1;
+        }
+      }
+    };
     if (m.kind == TASK_A1) {
       if (cur_phase_inst != m.inst) {
-        compute_sync();
         PhaseV<R>::stage(D.phase, phase_smem, tid, kComputeThreads);
-        compute_sync();
+        __syncthreads();
         if (tid == 0) cur_phase_inst = m.inst;
       }
-      process_a1<R, false>(tile, tile + kStageTileBytes, D, m.tile, m.step, phase_smem, red, &last_flag);
+      process_a1<R, false>(stage, stage + kStageTileBytes, D, m.tile, m.step, phase_smem, red, &last_flag,
+                           stage_free);
     } else if (m.kind == TASK_M) {
-      process_a1<R, true>(tile, tile + kStageTileBytes, D, m.tile, m.step, phase_smem, red, &last_flag);
+      process_a1<R, true>(stage, stage + kStageTileBytes, D, m.tile, m.step, phase_smem, red, &last_flag,
+                          stage_free);
     } else {
       const bool s2 = (m.kind == TASK_S2);
       const int w = s2 ? D.w2 : D.w3;
@@ -679,19 +720,85 @@ __global__ void __launch_bounds__(kPersistThreads, 1)
       const uint32_t cp = (uint32_t)(kElemBits - w);
       const uint32_t mid = m.tile & ((1u << mb) - 1u), hi = m.tile >> mb;
       const uint32_t tile_base = (mid << cp) | (hi << (h0 + (uint32_t)w));
-      process_s_dispatch<R>(w, tile, D.state, tile_base, h0, D.tan[m.step]);
+      process_s_dispatch<R>(w, stage, D.state, tile_base, h0, D.tan[m.step], stage_free);
     }
-    // completion: stores visible gpu-wide, then count the task and free the stage
-    __threadfence();
-    compute_sync();
+    __syncthreads();  // every store of this task is issued
+    bool pending = false;
     if (tid == 0) {
+      pending = (nxt.kind != TASK_END) && !early;
+      cur = nxt;
+      if (!decode_task<R>(P, g_after, nxt)) nxt.kind = TASK_END;
+    }
+    __syncthreads();  // publish cur
+    if (tid == 32) {
+      // completion of task m: the stores of every thread precede the barrier
+      // above; this gpu-scope fence releases them together with the counter
+      __threadfence();
       if (m.kind == TASK_A1) atomicAdd(D.a1_done + (m.tile >> D.w2), 1u);
       else if (m.kind == TASK_S2) atomicAdd(D.s2_done, 1u);
       else if (m.kind == TASK_S3) atomicAdd(D.s3_done, 1u);
-      mbar_arrive(smem_addr(&empty_bar[s]));
     }
-    ++use[s];
-    s ^= 1;
+    if (tid == 0 && pending) {
+      const InstDesc<R>& D2 = insts[cur.inst];
+      uint32_t target = 0;
+      const unsigned int* ctr = task_dep(D2, cur, target);
+      if (wait_counter(ctr, target, P)) {
+        issue_task_load(D2, cur, stage, fb);
+        inflight = 1;
+      } else {
+        // the failure is recorded; the others see the abort while waiting for the tile
+      }
+    }
+  }
+  // a load still in flight (issued early for a task that will not run) lands before exit
+  if (tid == 0 && inflight) mbar_wait_bounded(fb, phase, P.err);
+}
+
+// ---------------------------------------------------------------------------
+// Grid variant: one CTA per tile of one pass (kind = TASK_A1 / TASK_S2 /
+// TASK_S3 / TASK_M), no dependencies (the kernel boundary orders the passes).
+// Same tile arithmetic as the persistent engine; blockIdx.x is the tile.
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(kComputeThreads, 2)
+    tile_pass_kernel(const InstDesc<R>* __restrict__ insts, int kind, uint32_t step, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full_bar;
+  __shared__ int last_flag;
+  unsigned char* stage = smem;
+  unsigned char* phase_smem = smem + PersistSmem::kPhaseOff;
+  double* red = reinterpret_cast<double*>(smem + PersistSmem::kRedOff);
+  const int tid = threadIdx.x;
+  const uint32_t fb = smem_addr(&full_bar);
+  const InstDesc<R>& D = insts[0];
+  StageMeta m;
+  m.kind = kind;
+  m.inst = 0;
+  m.tile = blockIdx.x;
+  m.step = step;
+  if (tid == 0) {
+    mbar_init(fb, 1);
+    fence_barrier_init();
+  }
+  if (kind == TASK_A1) PhaseV<R>::stage(D.phase, phase_smem, tid, kComputeThreads);
+  __syncthreads();
+  if (tid == 0) issue_task_load(D, m, stage, fb);
+  const bool ok = mbar_wait_bounded(fb, 0, err);
+  if (__syncthreads_or(!ok)) return;
+  auto none = []() {};
+  if (kind == TASK_A1) {
+    process_a1<R, false>(stage, stage + kStageTileBytes, D, m.tile, step, phase_smem, red, &last_flag, none);
+  } else if (kind == TASK_M) {
+    process_a1<R, true>(stage, stage + kStageTileBytes, D, m.tile, step, phase_smem, red, &last_flag, none);
+  } else {
+    const bool s2 = (kind == TASK_S2);
+    const int w = s2 ? D.w2 : D.w3;
+    const int mb = s2 ? D.s2_mid_bits : D.s3_mid_bits;
+    const uint32_t h0 = s2 ? (uint32_t)kElemBits : (uint32_t)(kElemBits + D.w2);
+    const uint32_t cp = (uint32_t)(kElemBits - w);
+    const uint32_t mid = m.tile & ((1u << mb) - 1u), hi = m.tile >> mb;
+    const uint32_t tile_base = (mid << cp) | (hi << (h0 + (uint32_t)w));
+    process_s_dispatch<R>(w, stage, D.state, tile_base, h0, D.tan[step], none);
   }
 }
 

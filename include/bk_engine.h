@@ -116,6 +116,35 @@ typedef struct bk_evolve_params {
  * p_less[m], d_h[m], norm[m] (host arrays of length sum(measure); norm may be NULL). */
 int bk_evolve(bk_ctx* ctx, const bk_evolve_params* p, double* p_less, double* d_h, double* norm);
 
+/* ---- Batched evolution: many statevectors in one persistent launch ----
+ *
+ * Every instance has its own n, trap and field; all share dt, the step count and
+ * the measurement schedule. The tile tasks of all instances run in ONE
+ * persistent kernel (launched through a captured CUDA graph when use_graph is
+ * set), interleaved so that each statevector's A1 output is re-read from L2.
+ * Outputs are row-major [instance][measurement]. */
+typedef struct bk_batch_instance {
+  int32_t n;           /* qubits: 14..30 (complex64) or 13..30 (complex128) */
+  int32_t reserved;
+  uint64_t s0;         /* trap bits */
+  int64_t e0;          /* P_< threshold; < 0 means E(s0) */
+  double g_const;      /* field when g == NULL */
+  const double* g;     /* n_steps entries, or NULL */
+} bk_batch_instance;
+
+typedef struct bk_batch_params {
+  int32_t precision;   /* bk_precision */
+  int32_t n_steps;
+  double dt;
+  double diag_scale;   /* <= 0: 1/n of each instance */
+  const uint8_t* measure; /* n_steps + 1 flags, shared */
+  int32_t use_graph;   /* 1: launch through a captured CUDA graph */
+  int32_t lag;         /* task blocks between a slab's A1 and S2 tasks (<= 0: engine default) */
+} bk_batch_params;
+
+int bk_evolve_batch(bk_ctx* ctx, const bk_batch_params* p, const bk_batch_instance* inst, int32_t n_inst,
+                    double* p_less, double* d_h, double* norm);
+
 /* Copies the statevector left by the last bk_evolve to host as interleaved
  * (re, im) doubles, 2 * 2^n entries, in the requested ordering's convention. */
 int bk_export_state(bk_ctx* ctx, double* host_state_ri);
@@ -199,6 +228,14 @@ void bk_sampling_result_release(bk_sampling_result* r);
  * E(s)); n (or max_d + 1) when none exists or target <= E*(n)
  * (labs_energy.hpp:175-207). Hamming spheres are enumerated on the device. */
 int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* d_out);
+
+/* Engine options (tuning knobs; the autotuner sets them from its cache):
+ *   BK_OPT_ENGINE_MODE: 0 = persistent dataflow kernel (all steps in one launch,
+ *       L2 hand-off between the A1 and S2 tasks), 1 = one grid launch per pass;
+ *   BK_OPT_SLAB_LAG: persistent engine, slabs between A1 and S2 of a slab (>= 1). */
+enum { BK_OPT_ENGINE_MODE = 0, BK_OPT_SLAB_LAG = 1 };
+int bk_set_option(bk_ctx* ctx, int option, int64_t value);
+int bk_get_option(const bk_ctx* ctx, int option, int64_t* value);
 
 /* ---- Projective sampling (sampler.cuh:459-487, 559-598) ---- */
 
