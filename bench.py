@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
     ap.add_argument("--engine-mode", type=int, default=None, help="0 persistent, 1 one launch per pass")
+    ap.add_argument("--workload", choices=["large", "batched"], default="large",
+                    help="large: the N=28 headline; batched: 512 instances (64 traps x 8 g), N in {16,18,20,22}")
     ap.add_argument("--slab-lag", type=int, default=None)
     return ap.parse_args()
 
@@ -173,10 +175,84 @@ def run_reference(a):
     print(json.dumps(line))
 
 
+def batched_instances(seed=2024):
+    """64 traps (seeded descents, lowest 5% of 1000) with N drawn from {16,18,20,22}, x 8 g in [0.2, 0.5]."""
+    import bk_b200 as bk
+    rng = np.random.default_rng(seed)
+    traps = []
+    for j in range(64):
+        n = int(rng.choice([16, 18, 20, 22]))
+        bits, e0 = bk.select_trap(n, 42 + j, 1000, 0.05)
+        traps.append((n, bits, e0))
+    return [dict(n=n, s0=bits, e0=e0, g=float(g)) for (n, bits, e0) in traps for g in np.linspace(0.2, 0.5, 8)]
+
+
+def run_batched(a):
+    import torch
+    import bk_b200 as bk
+    steps_t = 500
+    dev = torch.device("cuda", 0)
+    eng = bk.Engine(0)
+    inst = batched_instances()
+    amp_steps = float(sum(1 << d["n"] for d in inst)) * steps_t
+    stream = torch.cuda.ExternalStream(eng.stream_handle(), device=dev)
+    meas = range(0, steps_t + 1)
+    for _ in range(max(a.warmup, 1)):
+        eng.evolve_batch(inst, a.dt, steps_t, measure=meas, precision=bk.BK_C64, use_graph=True)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clocks:
+        t0 = time.perf_counter()
+        ev0.record(stream)
+        for _ in range(a.steps):
+            p, d, nn = eng.evolve_batch(inst, a.dt, steps_t, measure=meas, precision=bk.BK_C64, use_graph=True)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - t0
+    dev_s = ev0.elapsed_time(ev1) / 1e3
+    value = amp_steps * a.steps / dev_s
+    # the same 512 instances one after another, each through its own launches
+    seq = {}
+    for mode in (1, 0):
+        eng.set_option("engine_mode", mode)
+        eng.evolve(inst[0]["n"], inst[0]["s0"], inst[0]["g"], a.dt, 4, measure=[0], e0=inst[0]["e0"])
+        torch.cuda.synchronize(dev)
+        e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0_.record(stream)
+        for d in inst:
+            eng.evolve(d["n"], d["s0"], d["g"], a.dt, steps_t, measure=meas, e0=d["e0"], precision=bk.BK_C64)
+        e1_.record(stream)
+        torch.cuda.synchronize(dev)
+        seq["sequential_" + ("one_launch_per_pass" if mode == 1 else "persistent_per_instance")] = \
+            amp_steps / (e0_.elapsed_time(e1_) / 1e3)
+    best_seq = max(seq.values())
+    line = {"metric": "Batched Trotter amp-steps/s (512 instances, N in {16,18,20,22}, complex64)", "value": value,
+            "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * dev_s / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64",
+            "data": "synthetic (64 seeded traps x 8 g, no dataset)",
+            "config": {"workload": "512 instances = 64 traps (lowest 5% of 1000 descents, N uniform in "
+                                   "{16,18,20,22}, seed 2024) x 8 g in linspace(0.2, 0.5, 8); dt=0.02, 500 Trotter "
+                                   "steps, P_< and <d_H> every step; one persistent launch through a captured "
+                                   "CUDA graph per bench step",
+                       "instances": len(inst), "trotter_steps_per_step": steps_t,
+                       "amp_steps_per_step": amp_steps},
+            "compare": dict(seq, batched_over_best_sequential=value / best_seq),
+            "e2e": {"value": amp_steps * a.steps / wall, "unit": UNIT, "h2d_bytes_per_step": 24 * len(inst) + 501,
+                    "d2h_bytes_per_step": 3 * 8 * len(inst) * 501},
+            "clocks": clocks.summary(),
+            "check": {"p_less_mean_last": float(np.mean(p[:, -1])), "norm_max_dev": float(np.max(np.abs(nn - 1)))}}
+    eng.close()
+    print(json.dumps(line))
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+        return
+    if a.workload == "batched":
+        run_batched(a)
         return
     import torch
     import torch.distributed as dist
