@@ -52,6 +52,9 @@ def lib():
         L.orc_trotter_evolve.restype = ctypes.c_int
         L.orc_trotter_evolve.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, dp, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, u8p, dp, dp, dp, ctypes.c_int, dp, dp]
+        L.orc_trotter_adjoint.restype = ctypes.c_int
+        L.orc_trotter_adjoint.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, dp, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
         L.orc_sample_indices.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int64, u64p]
         L.orc_uniform_randoms.argtypes = [ctypes.c_uint64, ctypes.c_int64, dp]
         L.orc_sampler_run.restype = ctypes.c_int
@@ -154,6 +157,27 @@ def trotter_evolve(n, s0, e0, g, dt, n_steps, measure=None, diag_scale=0.0, thre
     if want_state:
         return p, d, nn, st[0::2] + 1j * st[1::2]
     return p, d, nn
+
+
+def segment_steps(n_steps, n_segments):
+    """Step -> segment map of a piecewise-constant schedule with equal segments."""
+    if n_segments <= 0 or n_steps % n_segments:
+        raise ValueError("n_steps must be a multiple of n_segments")
+    return np.repeat(np.arange(n_segments), n_steps // n_segments)
+
+
+def trotter_adjoint(n, s0, e0, g, dt, n_steps, objective=0, diag_scale=0.0, threads=0):
+    """Adjoint gradient of O(T) (0: P_<, 1: <d_H>) w.r.t. the per-step field g_k.
+
+    Returns (O, dO/dg_k for k < n_steps); complex128, exact gates."""
+    g_arr = np.ascontiguousarray(np.broadcast_to(np.asarray(g, dtype=np.float64), (max(n_steps, 1),)))
+    grad = np.zeros(max(n_steps, 1))
+    val = np.zeros(1)
+    rc = lib().orc_trotter_adjoint(n, s0, e0, _ptr(g_arr, dp), dt, diag_scale, n_steps, objective, threads,
+                                   _ptr(val, dp), _ptr(grad, dp))
+    if rc != 0:
+        raise ValueError(f"orc_trotter_adjoint rejected n={n}, n_steps={n_steps}, objective={objective}")
+    return float(val[0]), grad[:n_steps]
 
 
 def sample_indices(n, state, randnums):

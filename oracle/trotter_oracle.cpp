@@ -286,6 +286,158 @@ int orc_trotter_evolve(int n, uint64_t s0, int64_t e0, const double* g_per_step,
   return 0;
 }
 
+}  // extern "C"
+
+namespace {
+
+using cvec = std::vector<std::complex<double>>;
+
+// One reference-order Trotter step psi <- M(g) D psi, exact gates as in
+// orc_trotter_evolve (sampler.cuh:73-91 phase, :451-457 + :611-617 mixer).
+void trotter_step(cvec& psi, const std::vector<uint16_t>& E, int n, double angle_unit, double g, double dt) {
+  const int64_t A = (int64_t)psi.size();
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < A; ++s) {
+    const double th = -angle_unit * (double)E[(size_t)s];
+    psi[(size_t)s] *= std::complex<double>(std::cos(th), std::sin(th));
+  }
+  const double c = std::cos(g * dt), sn = std::sin(g * dt);
+  const std::complex<double> m00(c, 0.0), m01(0.0, sn);
+  for (int q = 0; q < n; ++q) {
+    const int64_t bit = 1LL << q;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < A / 2; ++i) {
+      const int64_t a = ((i >> q) << (q + 1)) | (i & (bit - 1));
+      const int64_t b = a | bit;
+      const std::complex<double> x = psi[(size_t)a], y = psi[(size_t)b];
+      psi[(size_t)a] = m00 * x + m01 * y;
+      psi[(size_t)b] = m01 * x + m00 * y;
+    }
+  }
+}
+
+// The adjoint step lambda <- (M(g) D)^dagger lambda = D^dagger M(-g) lambda.
+void adjoint_step(cvec& lam, const std::vector<uint16_t>& E, int n, double angle_unit, double g, double dt) {
+  const int64_t A = (int64_t)lam.size();
+  const double c = std::cos(g * dt), sn = -std::sin(g * dt);
+  const std::complex<double> m00(c, 0.0), m01(0.0, sn);
+  for (int q = 0; q < n; ++q) {
+    const int64_t bit = 1LL << q;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < A / 2; ++i) {
+      const int64_t a = ((i >> q) << (q + 1)) | (i & (bit - 1));
+      const int64_t b = a | bit;
+      const std::complex<double> x = lam[(size_t)a], y = lam[(size_t)b];
+      lam[(size_t)a] = m00 * x + m01 * y;
+      lam[(size_t)b] = m01 * x + m00 * y;
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < A; ++s) {
+    const double th = angle_unit * (double)E[(size_t)s];
+    lam[(size_t)s] *= std::complex<double>(std::cos(th), std::sin(th));
+  }
+}
+
+// Im <lam| G |psi> with G = sum_q X_q, summed in a fixed order.
+double im_lam_g_psi(const cvec& lam, const cvec& psi, int n) {
+  const int64_t A = (int64_t)psi.size();
+  const int64_t nblk = std::min<int64_t>(A, 1024);
+  std::vector<double> part((size_t)nblk, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t b = 0; b < nblk; ++b) {
+    const int64_t lo = A * b / nblk, hi = A * (b + 1) / nblk;
+    double acc = 0.0;
+    for (int64_t s = lo; s < hi; ++s) {
+      std::complex<double> gp(0.0, 0.0);
+      for (int q = 0; q < n; ++q) gp += psi[(size_t)(s ^ (1LL << q))];
+      acc += (std::conj(lam[(size_t)s]) * gp).imag();
+    }
+    part[(size_t)b] = acc;
+  }
+  double tot = 0.0;
+  for (double v : part) tot += v;
+  return tot;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Gradient of a diagonal observable at the final time with respect to the
+// per-step transverse field, by the adjoint method. The reference has no
+// gradient; this restates the textbook derivation for its step
+// psi_{k+1} = M(g_k) D psi_k (sampler.cuh:604-618) with
+// M(g) = prod_q exp(+i g dt X_q), dM/dg = i dt G M, G = sum_q X_q:
+//   O = <psi_T| W |psi_T>,  lambda_T = W psi_T,  lambda_k = (M(g_k) D)^dagger lambda_{k+1},
+//   dO/dg_k = 2 Re <lambda_{k+1}| i dt G |psi_{k+1}> = -2 dt Im <lambda_{k+1}| G |psi_{k+1}>.
+// W = [E(s) < e0] (objective 0, P_<) or popcount(s ^ s0) (objective 1, <d_H>).
+// The forward states psi_{k+1} are recomputed from checkpoints every C ~ sqrt(T)
+// steps (exact gates, no inverse steps), so this checker shares no numerical
+// shortcut with the device adjoint. grad_out[k] = dO/dg_k for k < n_steps.
+int orc_trotter_adjoint(int n, uint64_t s0, int64_t e0, const double* g_per_step, double dt, double diag_scale,
+                        int n_steps, int objective, int n_threads, double* value_out, double* grad_out) {
+  if (n < 1 || n > 26 || n_steps < 0 || (objective != 0 && objective != 1)) return 1;
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+  const int64_t A = 1LL << n;
+  s0 &= mask_of(n);
+  std::vector<uint16_t> E((size_t)A);
+  orc_energy_table_u16(n, E.data());
+  const double angle_unit = (diag_scale > 0.0) ? (dt * diag_scale) : (dt / (double)n);
+  const int C = std::max(1, (int)std::ceil(std::sqrt((double)std::max(n_steps, 1))));
+  // forward with checkpoints psi_{jC}
+  std::vector<cvec> ckpt;
+  cvec psi((size_t)A, {0.0, 0.0});
+  psi[(size_t)s0] = {1.0, 0.0};
+  for (int k = 0; k < n_steps; ++k) {
+    if (k % C == 0) ckpt.push_back(psi);
+    trotter_step(psi, E, n, angle_unit, g_per_step[k], dt);
+  }
+  // objective and lambda_T = W psi_T
+  cvec lam((size_t)A);
+  double value = 0.0;
+  {
+    const int64_t nblk = std::min<int64_t>(A, 1024);
+    std::vector<double> part((size_t)nblk, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < nblk; ++b) {
+      const int64_t lo = A * b / nblk, hi = A * (b + 1) / nblk;
+      double acc = 0.0;
+      for (int64_t s = lo; s < hi; ++s) {
+        const double w = (objective == 0) ? (((int64_t)E[(size_t)s] < e0) ? 1.0 : 0.0)
+                                          : (double)__builtin_popcountll((uint64_t)s ^ s0);
+        lam[(size_t)s] = w * psi[(size_t)s];
+        acc += w * std::norm(psi[(size_t)s]);
+      }
+      part[(size_t)b] = acc;
+    }
+    for (double v : part) value += v;
+  }
+  if (value_out) *value_out = value;
+  // reverse sweep window by window; psi_{k+1} recomputed forward inside the window
+  for (int w = (int)ckpt.size() - 1; w >= 0; --w) {
+    const int k0 = w * C, k1 = std::min(n_steps, k0 + C);
+    std::vector<cvec> traj;  // psi_{k0+1} .. psi_{k1}
+    cvec x = ckpt[(size_t)w];
+    for (int k = k0; k < k1; ++k) {
+      trotter_step(x, E, n, angle_unit, g_per_step[k], dt);
+      traj.push_back(x);
+    }
+    for (int k = k1 - 1; k >= k0; --k) {
+      // lam = lambda_{k+1}, traj[k - k0] = psi_{k+1}
+      grad_out[k] = -2.0 * dt * im_lam_g_psi(lam, traj[(size_t)(k - k0)], n);
+      adjoint_step(lam, E, n, angle_unit, g_per_step[k], dt);
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"
+
+extern "C" {
+
 // Projective sampling by inverse CDF over |psi|^2 (the reference delegates to the
 // closed cuStateVec sampler, sampler.cuh:464-466, 564-573; output in random-number
 // order): shot k returns the smallest index s with u_k * total < cdf(s), where
