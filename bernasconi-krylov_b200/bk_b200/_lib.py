@@ -12,6 +12,7 @@ BK_OK, BK_ERR_INVALID, BK_ERR_CUDA, BK_ERR_OOM, BK_ERR_TIMEOUT, BK_ERR_NORM, BK_
 BK_C64, BK_C128 = 0, 1
 BK_FUSED, BK_PLAIN = 0, 1
 BK_ORDER_REFERENCE, BK_ORDER_STRANG = 0, 1
+BK_OBJ_P_LESS, BK_OBJ_D_H = 0, 1
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _u16p = ctypes.POINTER(ctypes.c_uint16)
@@ -45,6 +46,19 @@ class BatchParamsC(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("n_steps", ctypes.c_int32), ("dt", ctypes.c_double),
                 ("diag_scale", ctypes.c_double), ("measure", _u8p), ("use_graph", ctypes.c_int32),
                 ("lag", ctypes.c_int32)]
+
+
+class AdjointParamsC(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("precision", ctypes.c_int32), ("s0", ctypes.c_uint64), ("e0", ctypes.c_int64),
+                ("dt", ctypes.c_double), ("diag_scale", ctypes.c_double), ("n_steps", ctypes.c_int32),
+                ("n_segments", ctypes.c_int32), ("g", _dp), ("segment_of_step", ctypes.POINTER(ctypes.c_int32)),
+                ("checkpoint_every", ctypes.c_int32), ("objective", ctypes.c_int32)]
+
+
+class AdjointStatsC(ctypes.Structure):
+    _fields_ = [("value", ctypes.c_double), ("norm", ctypes.c_double), ("checkpoint_every", ctypes.c_int32),
+                ("n_checkpoints", ctypes.c_int32), ("max_drift", ctypes.c_double), ("forward_ms", ctypes.c_double),
+                ("reverse_ms", ctypes.c_double)]
 
 
 class SamplerConfigC(ctypes.Structure):
@@ -116,6 +130,7 @@ def load_library(build_if_missing=True):
     L.bk_evolve_batch.argtypes = [c_ctx, ctypes.POINTER(BatchParamsC), ctypes.POINTER(BatchInstanceC), ctypes.c_int32,
                                   _dp, _dp, _dp]
     L.bk_get_option.argtypes = [c_ctx, ctypes.c_int, _i64p]
+    L.bk_adjoint.argtypes = [c_ctx, ctypes.POINTER(AdjointParamsC), _dp, _dp, _dp, ctypes.POINTER(AdjointStatsC)]
     L.bk_sampler_run.argtypes = [c_ctx, ctypes.POINTER(SamplerConfigC), ctypes.c_uint64,
                                  ctypes.POINTER(SamplingResultC)]
     L.bk_sampling_result_release.argtypes = [ctypes.POINTER(SamplingResultC)]
@@ -277,6 +292,33 @@ class Engine:
         self._check(self.L.bk_evolve_batch(self.ctx, ctypes.byref(bp), arr, len(instances), _p(p, _dp), _p(d, _dp),
                                            _p(nn, _dp)), "bk_evolve_batch")
         return p, d, nn
+
+    def adjoint(self, n, s0, g_segments, dt, n_steps, segment_of_step=None, e0=-1, precision=BK_C64,
+                objective=BK_OBJ_P_LESS, checkpoint_every=128, diag_scale=0.0, per_step=False):
+        """O(T) and dO/dg_j of a piecewise-constant field schedule (adjoint method).
+
+        Returns (value, grad[n_segments], stats dict); with ``per_step`` the stats
+        also carry ``grad_steps`` (dO/dg_k for every step)."""
+        g = np.ascontiguousarray(g_segments, dtype=np.float64)
+        seg = None
+        if segment_of_step is not None:
+            seg = np.ascontiguousarray(segment_of_step, dtype=np.int32)
+            if len(seg) != n_steps:
+                raise ValueError("segment_of_step must have n_steps entries")
+        ap = AdjointParamsC(n=n, precision=precision, s0=s0, e0=e0, dt=dt, diag_scale=diag_scale, n_steps=n_steps,
+                            n_segments=len(g), g=_p(g, _dp),
+                            segment_of_step=_p(seg, ctypes.POINTER(ctypes.c_int32)),
+                            checkpoint_every=checkpoint_every, objective=objective)
+        val = np.zeros(1)
+        grad = np.zeros(len(g))
+        gsteps = np.zeros(max(n_steps, 1)) if per_step else None
+        st = AdjointStatsC()
+        self._check(self.L.bk_adjoint(self.ctx, ctypes.byref(ap), _p(val, _dp), _p(grad, _dp), _p(gsteps, _dp),
+                                      ctypes.byref(st)), "bk_adjoint")
+        stats = {k: getattr(st, k) for k, _ in AdjointStatsC._fields_}
+        if per_step:
+            stats["grad_steps"] = gsteps[:n_steps]
+        return float(val[0]), grad, stats
 
     def d_min(self, n, bits, target=-1, max_d=-1):
         d = ctypes.c_int()

@@ -19,6 +19,7 @@
 #include <unordered_set>
 #include <vector>
 
+#include "bk_adjoint.cuh"
 #include "bk_aux.cuh"
 #include "bk_engine.h"
 #include "bk_fused.cuh"
@@ -95,6 +96,12 @@ struct bk_ctx {
   size_t batch_cap = 0;
   double* d_batch_results = nullptr;
   size_t batch_results_cap = 0;
+  void* d_lam = nullptr;      // adjoint: lambda statevector
+  size_t lam_cap = 0;
+  void* d_ckpt = nullptr;     // adjoint: checkpoints of psi
+  size_t ckpt_cap = 0;
+  void* d_adj = nullptr;      // adjoint: maps, descriptor, per-step arrays, partials
+  size_t adj_cap = 0;
   // tensor maps, keyed by (state ptr, n, precision, pass)
   std::map<std::string, TmaDesc> tma;
   // last evolution (for export / sampling)
@@ -588,9 +595,26 @@ struct Bump {
   }
 };
 
+// A prepared persistent-engine run over c->d_state: device buffers laid out,
+// tasks and per-step arrays uploaded; persist_launch runs any range of steps.
 template <class R>
-int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double angle_unit,
-                   const std::vector<R>& tans, const std::vector<R>& scales) {
+struct PersistRun {
+  char* base = nullptr;
+  size_t o_desc = 0, o_tasks = 0, o_final = 0, o_tan = 0, o_scale = 0, o_slot = 0;
+  InstDesc<R> D{};
+  unsigned int* ctr = nullptr;
+  uint32_t slabs = 0;
+  size_t n_tasks = 0, n_final = 0;
+  unsigned int* next = nullptr;
+  int* err = nullptr;
+  int* abort_w = nullptr;
+  uint32_t n_a1 = 0, n_s2 = 0, n_s3 = 0;
+  typename PhaseV<R>::params phase{};  // device tables of the diagonal phase
+};
+
+template <class R>
+int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double angle_unit,
+                    const std::vector<R>& tans, const std::vector<R>& scales, PersistRun<R>* run) {
   const int n = p->n;
   const bool c64 = sizeof(R) == 4;
   const int np = c64 ? n - 1 : n;  // element bits
@@ -720,6 +744,78 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
   if (!hab.empty())
     BK_CUDA(c, cudaMemcpyAsync(base + o_hab, hab.data(), hab.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
   BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R>), PersistSmem::kBytes));
+  run->base = base;
+  run->o_desc = o_desc;
+  run->o_tasks = o_tasks;
+  run->o_final = o_final;
+  run->o_tan = o_tan;
+  run->o_scale = o_scale;
+  run->o_slot = o_slot;
+  run->D = D;
+  run->ctr = ctr;
+  run->slabs = slabs;
+  run->n_tasks = tasks.size();
+  run->n_final = final_tasks.size();
+  run->next = next;
+  run->err = err;
+  run->abort_w = abort_w;
+  run->n_a1 = n_a1;
+  run->n_s2 = n_s2;
+  run->n_s3 = n_s3;
+  run->phase = D.phase;
+  return BK_OK;
+}
+
+// Steps [k0, k0 + n_steps) in one persistent launch, then `n_final`
+// measurement-only tasks (0 or all of them) for step k0 + n_steps; waits for the
+// launch and reports a bounded device wait that gave up.
+template <class R>
+int persist_launch(bk_ctx* c, PersistRun<R>& r, int k0, int n_steps, size_t n_final) {
+  cudaStream_t st = c->stream;
+  InstDesc<R> D = r.D;
+  D.tan = reinterpret_cast<const R*>(r.base + r.o_tan) + k0;
+  D.scale = reinterpret_cast<const R*>(r.base + r.o_scale) + k0;
+  D.slot = reinterpret_cast<const int*>(r.base + r.o_slot) + k0;
+  BK_CUDA(c, cudaMemcpyAsync(r.base + r.o_desc, &D, sizeof(D), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemsetAsync(r.ctr, 0, (r.slabs + 8) * sizeof(unsigned int), st));
+  Program P{};
+  P.tasks = reinterpret_cast<const unsigned long long*>(r.base + r.o_tasks);
+  P.per_step = (uint32_t)r.n_tasks;
+  P.n_steps = (uint32_t)n_steps;
+  P.final_tasks = reinterpret_cast<const unsigned long long*>(r.base + r.o_final);
+  P.n_final = (uint32_t)n_final;
+  P.step0 = (uint32_t)k0;
+  P.next = r.next;
+  P.err = r.err;
+  P.abort = r.abort_w;
+  if (P.n_steps == 0 && P.n_final == 0) return BK_OK;
+  size_t ev = 0;
+  BK_TRY(ev_begin(c, "persist", &ev));
+  persist_kernel<R><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
+      reinterpret_cast<const InstDesc<R>*>(r.base + r.o_desc), P);
+  BK_CUDA(c, cudaGetLastError());
+  BK_TRY(ev_end(c, ev));
+  int e = 0;
+  BK_CUDA(c, cudaMemcpyAsync(&e, r.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  BK_CUDA(c, cudaStreamSynchronize(st));
+  if (e != 0) return fail(c, BK_ERR_TIMEOUT, "persistent engine: a bounded device wait gave up (%d)", e);
+  return BK_OK;
+}
+
+template <class R>
+int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double angle_unit,
+                   const std::vector<R>& tans, const std::vector<R>& scales) {
+  PersistRun<R> run;
+  BK_TRY(persist_prepare<R>(c, p, S, angle_unit, tans, scales, &run));
+  const int n = p->n;
+  cudaStream_t st = c->stream;
+  char* base = run.base;
+  unsigned int* ctr = run.ctr;
+  const uint32_t slabs = run.slabs;
+  int* err = run.err;
+  const uint32_t n_a1 = run.n_a1, n_s2 = run.n_s2, n_s3 = run.n_s3;
+  const size_t o_desc = run.o_desc;
+  InstDesc<R> D = run.D;
 
   if (c->engine_mode == 1) {
     // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end
@@ -770,54 +866,15 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
     int k1 = search;
     while (k1 < p->n_steps && S.sample_pt[(size_t)k1] < 0) ++k1;
     // launch steps [k0, k1) (+ the final measurement when k1 == n_steps)
-    D.tan = reinterpret_cast<const R*>(base + o_tan) + k0;
-    D.scale = reinterpret_cast<const R*>(base + o_scale) + k0;
-    D.slot = reinterpret_cast<const int*>(base + o_slot) + k0;
-    BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &D, sizeof(D), cudaMemcpyHostToDevice, st));
-    BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
-    Program P{};
-    P.tasks = reinterpret_cast<const unsigned long long*>(base + o_tasks);
-    P.per_step = (uint32_t)tasks.size();
-    P.n_steps = (uint32_t)(k1 - k0);
     const bool last = (k1 == p->n_steps);
     const bool sample_final = last && S.sample_pt[(size_t)k1] >= 0;
-    P.final_tasks = reinterpret_cast<const unsigned long long*>(base + o_final);
-    P.n_final = (last && !sample_final) ? (uint32_t)final_tasks.size() : 0u;
-    P.step0 = (uint32_t)k0;
-    P.next = next;
-    P.err = err;
-    P.abort = abort_w;
-    if (P.n_steps > 0 || P.n_final > 0) {
-      size_t ev = 0;
-      BK_TRY(ev_begin(c, "persist", &ev));
-      persist_kernel<R><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
-          reinterpret_cast<const InstDesc<R>*>(base + o_desc), P);
-      BK_CUDA(c, cudaGetLastError());
-      BK_TRY(ev_end(c, ev));
-      int e = 0;
-      BK_CUDA(c, cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
-      BK_CUDA(c, cudaStreamSynchronize(st));
-      if (e != 0) return fail(c, BK_ERR_TIMEOUT, "persistent engine: a bounded device wait gave up (%d)", e);
-    }
+    BK_TRY(persist_launch<R>(c, run, k0, k1 - k0, (last && !sample_final) ? run.n_final : 0));
     if (k1 >= p->n_steps && !sample_final) break;
     // sampling point k1 (state psi_k1 is in place)
     BK_TRY(launch_sampling_t(c, reinterpret_cast<const Samp*>(c->d_state), n, S.sample_pt[(size_t)k1], S.shots));
     if (sample_final) {
       // final measurement after sampling
-      if (!final_tasks.empty()) {
-        D.slot = reinterpret_cast<const int*>(base + o_slot) + k1;
-        BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &D, sizeof(D), cudaMemcpyHostToDevice, st));
-        BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
-        P.n_steps = 0;
-        P.n_final = (uint32_t)final_tasks.size();
-        size_t ev = 0;
-        BK_TRY(ev_begin(c, "persist", &ev));
-        persist_kernel<R><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
-            reinterpret_cast<const InstDesc<R>*>(base + o_desc), P);
-        BK_CUDA(c, cudaGetLastError());
-        BK_TRY(ev_end(c, ev));
-        BK_CUDA(c, cudaStreamSynchronize(st));
-      }
+      BK_TRY(persist_launch<R>(c, run, k1, 0, run.n_final));
       break;
     }
     k0 = k1;
@@ -1306,6 +1363,285 @@ int evolve_plain(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
   return BK_OK;
 }
 
+// ---------------------------------------------------------------------------
+// adjoint gradient (csrc/bk_adjoint.cuh)
+// ---------------------------------------------------------------------------
+constexpr int kResetGrid = 148 * 4;
+
+// Forward run with checkpoints every K steps (persistent engine), lambda_T = W
+// psi_T, then the reverse sweep: per reverse step one dual A1 / S2 / S3 launch
+// each, a checkpoint put back every K steps. grad_step[k] = dO/dg_k.
+template <class R>
+int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& g_step, int64_t e0,
+              double angle_unit, int K, int n_ckpt, double* value_out, std::vector<double>* grad_step,
+              bk_adjoint_stats* stats) {
+  const int n = p->n, T = p->n_steps;
+  constexpr bool kC64 = sizeof(R) == 4;
+  const int np = kC64 ? n - 1 : n;
+  const size_t n_el = 1ull << np;
+  const size_t sbytes = n_el * 16;
+  cudaStream_t st = c->stream;
+  const uint32_t s0 = (uint32_t)(p->s0 & ((1ull << n) - 1ull));
+
+  // forward schedule (measurement at T only) and the host scale bookkeeping
+  Schedule S;
+  S.g = g_step;
+  S.slot.assign((size_t)T + 1, -1);
+  S.slot[(size_t)T] = 0;
+  S.n_meas = 1;
+  S.sample_pt.assign((size_t)T + 1, -1);
+  std::vector<R> tans((size_t)T), scales((size_t)T);
+  std::vector<long double> lgf((size_t)T + 1, 0.0L);
+  long double lg = 0.0L;
+  for (int k = 0; k <= T; ++k) {
+    lgf[(size_t)k] = lg;
+    if (k == T) break;
+    tans[(size_t)k] = (R)std::tan(g_step[(size_t)k] * p->dt);
+    R sc = (R)1;
+    if (lg >= (long double)kRescaleLog2) {
+      sc = (R)std::ldexp(1.0, -kRescaleLog2);
+      lg -= (long double)kRescaleLog2;
+    }
+    scales[(size_t)k] = sc;
+    const long double tf = (long double)tans[(size_t)k];
+    lg += 0.5L * (long double)n * std::log2(1.0L + tf * tf);
+  }
+  bk_evolve_params q{};
+  q.n = n;
+  q.precision = p->precision;
+  q.method = BK_FUSED;
+  q.s0 = p->s0;
+  q.e0 = e0;
+  q.dt = p->dt;
+  q.diag_scale = p->diag_scale;
+  q.n_steps = T;
+
+  BK_CUDA(c, cudaMemsetAsync(c->d_state, 0, sbytes, st));
+  if constexpr (kC64)
+    set_basis_planar_kernel<<<1, 1, 0, st>>>(reinterpret_cast<float*>(c->d_state), s0);
+  else
+    set_basis_kernel<double2><<<1, 1, 0, st>>>(reinterpret_cast<double2*>(c->d_state), s0);
+  BK_CUDA(c, cudaGetLastError());
+  c->planar = kC64;
+  c->have_state = false;
+
+  cudaEvent_t ev[4];
+  for (auto& e : ev) BK_CUDA(c, cudaEventCreate(&e));
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]);
+    }
+  } guard{ev};
+
+  PersistRun<R> run;
+  BK_TRY(persist_prepare<R>(c, &q, S, angle_unit, tans, scales, &run));
+  unsigned char* ckpt = static_cast<unsigned char*>(c->d_ckpt);
+  BK_CUDA(c, cudaEventRecord(ev[0], st));
+  for (int w = 0; w <= n_ckpt; ++w) {
+    const int k0 = w * K, k1 = (w == n_ckpt) ? T : (w + 1) * K;
+    if (w > 0)
+      BK_CUDA(c, cudaMemcpyAsync(ckpt + (size_t)(w - 1) * sbytes, c->d_state, sbytes, cudaMemcpyDeviceToDevice, st));
+    BK_TRY(persist_launch<R>(c, run, k0, k1 - k0, (w == n_ckpt) ? run.n_final : 0));
+  }
+  BK_CUDA(c, cudaEventRecord(ev[1], st));
+  double row[4] = {0, 0, 0, 0};
+  BK_CUDA(c, cudaMemcpyAsync(row, c->d_results, sizeof(row), cudaMemcpyDeviceToHost, st));
+  BK_CUDA(c, cudaStreamSynchronize(st));
+  const long double f = std::exp2(-2.0L * lgf[(size_t)T]);
+  const double value = (double)((long double)row[p->objective == BK_OBJ_P_LESS ? 0 : 1] * f);
+  if (value_out) *value_out = value;
+  grad_step->assign((size_t)T, 0.0);
+  float fw_ms = 0.f;
+  BK_CUDA(c, cudaEventElapsedTime(&fw_ms, ev[0], ev[1]));
+  if (stats) {
+    stats->value = value;
+    stats->norm = (double)((long double)row[2] * f);
+    stats->checkpoint_every = K;
+    stats->n_checkpoints = n_ckpt;
+    stats->max_drift = 0.0;
+    stats->forward_ms = fw_ms;
+    stats->reverse_ms = 0.0;
+  }
+  if (T == 0) return BK_OK;
+
+  // reverse-sweep bookkeeping on the host: tangents, rescales, round-weight
+  // logs, the log2 scale of both vectors at each step's cross terms, resets
+  const InstDesc<R>& FD = run.D;
+  const int w2 = FD.w2, w3 = FD.w3;
+  std::vector<R> t_rev((size_t)T), sc_rev((size_t)T);
+  std::vector<double> lg_rev((size_t)T);
+  std::vector<long double> wlog2((size_t)T);
+  struct Reset {
+    int after_j, ck;
+    double a, b;
+  };
+  std::vector<Reset> resets;
+  long double lp = lgf[(size_t)T], ll = lgf[(size_t)T];
+  for (int j = 0; j < T; ++j) {
+    const int k = T - 1 - j;
+    R sc = (R)1;
+    if (std::max(lp, ll) >= (long double)kRescaleLog2) {
+      sc = (R)std::ldexp(1.0, -kRescaleLog2);
+      lp -= (long double)kRescaleLog2;
+      ll -= (long double)kRescaleLog2;
+    }
+    sc_rev[(size_t)j] = sc;
+    t_rev[(size_t)j] = -tans[(size_t)k];
+    const long double tf = (long double)tans[(size_t)k];
+    const long double l2 = std::log2(1.0L + tf * tf);
+    lg_rev[(size_t)j] = (double)l2;
+    wlog2[(size_t)j] = lp + ll;
+    lp += 0.5L * (long double)n * l2;
+    ll += 0.5L * (long double)n * l2;
+    if (k > 0 && k % K == 0) {
+      const int m = k / K;  // checkpoint m - 1 holds psi_k
+      resets.push_back(Reset{j, m - 1, (double)std::exp2(-lp), (double)std::exp2(-lgf[(size_t)k])});
+      lp = lgf[(size_t)k];
+    }
+  }
+
+  // device layout
+  const uint32_t n_a1 = FD.n_a1, n_s2 = FD.n_s2, n_s3 = FD.n_s3;
+  Bump b;
+  const size_t o_maps = b.take(7 * sizeof(CUtensorMap));
+  const size_t o_desc = b.take(sizeof(AdjDesc<R>));
+  const size_t o_tan = b.take((size_t)T * sizeof(R));
+  const size_t o_sc = b.take((size_t)T * sizeof(R));
+  const size_t o_lg = b.take((size_t)T * sizeof(double));
+  const size_t o_part = b.take((size_t)(n_a1 + n_s2 + n_s3) * sizeof(double));
+  const size_t o_ctr = b.take(64);
+  const size_t o_cross = b.take((size_t)T * sizeof(double));
+  const size_t o_dev = b.take(std::max<size_t>(resets.size(), 1) * kResetGrid * sizeof(double));
+  BK_TRY(ensure_buffer(c, &c->d_adj, &c->adj_cap, b.off));
+  char* base = static_cast<char*>(c->d_adj);
+  CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(base + o_maps);
+  unsigned int* ticket = reinterpret_cast<unsigned int*>(base + o_ctr);
+  int* err = reinterpret_cast<int*>(base + o_ctr + 16);
+  double* d_cross = reinterpret_cast<double*>(base + o_cross);
+  double* d_dev = reinterpret_cast<double*>(base + o_dev);
+
+  TmaDesc a1p, a1l, em, s2p, s2l, s3p, s3l;
+  BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits, kElemBits, 0, &a1p));
+  BK_TRY(build_amp_map(c, c->d_lam, np, BK_C128, kElemBits, kElemBits, 0, &a1l));
+  BK_TRY(build_e_map(c, c->d_E, n, kC64 ? 13 : 12, &em));
+  BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w2, kElemBits, w2, &s2p));
+  BK_TRY(build_amp_map(c, c->d_lam, np, BK_C128, kElemBits - w2, kElemBits, w2, &s2l));
+  if (w3 > 0) {
+    BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w3, kElemBits + w2, w3, &s3p));
+    BK_TRY(build_amp_map(c, c->d_lam, np, BK_C128, kElemBits - w3, kElemBits + w2, w3, &s3l));
+  } else {
+    s3p = s2p;
+    s3l = s2l;
+  }
+  CUtensorMap maps[7] = {a1p.map, a1l.map, em.map, s2p.map, s2l.map, s3p.map, s3l.map};
+  AdjDesc<R> A{};
+  A.psi = static_cast<unsigned char*>(c->d_state);
+  A.lam = static_cast<unsigned char*>(c->d_lam);
+  A.map_a1 = d_maps + 0;
+  A.map_e = d_maps + 2;
+  A.map_s2 = d_maps + 3;
+  A.map_s3 = d_maps + 5;
+  A.np = np;
+  A.n = n;
+  A.w2 = w2;
+  A.w3 = w3;
+  A.a1_hi_dim = a1p.hi_dim;
+  A.s2_mid_dim = s2p.mid_dim;
+  A.s2_hi_dim = s2p.hi_dim;
+  A.s2_mid_bits = (int)s2p.mid_bits;
+  A.s3_mid_dim = w3 > 0 ? s3p.mid_dim : -1;
+  A.s3_hi_dim = w3 > 0 ? s3p.hi_dim : -1;
+  A.s3_mid_bits = w3 > 0 ? (int)s3p.mid_bits : 0;
+  A.phase = run.phase;
+  A.tan = reinterpret_cast<const R*>(base + o_tan);
+  A.scale = reinterpret_cast<const R*>(base + o_sc);
+  A.lg1t2 = reinterpret_cast<const double*>(base + o_lg);
+  A.partials = reinterpret_cast<double*>(base + o_part);
+  A.ticket = ticket;
+  A.cross = d_cross;
+  A.n_a1 = n_a1;
+  A.n_s2 = n_s2;
+  A.n_s3 = n_s3;
+  BK_CUDA(c, cudaMemcpyAsync(d_maps, maps, sizeof(maps), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &A, sizeof(A), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemcpyAsync(base + o_tan, t_rev.data(), (size_t)T * sizeof(R), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemcpyAsync(base + o_sc, sc_rev.data(), (size_t)T * sizeof(R), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemcpyAsync(base + o_lg, lg_rev.data(), (size_t)T * sizeof(double), cudaMemcpyHostToDevice, st));
+  BK_CUDA(c, cudaMemsetAsync(base + o_ctr, 0, 64, st));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(adj_pass_kernel<R>), AdjSmem::kBytes));
+  const AdjDesc<R>* dd = reinterpret_cast<const AdjDesc<R>*>(base + o_desc);
+  const int ns = c->num_sms;
+  const unsigned g1 = std::min<unsigned>(n_a1, (unsigned)ns), g2 = std::min<unsigned>(n_s2, (unsigned)ns),
+                 g3 = std::min<unsigned>(std::max<unsigned>(n_s3, 1u), (unsigned)ns);
+
+  BK_CUDA(c, cudaEventRecord(ev[2], st));
+  {
+    const unsigned grid = (unsigned)std::min<size_t>((n_el + 255) / 256, (size_t)kResetGrid);
+    adj_lambda_init_kernel<R><<<grid, 256, 0, st>>>(static_cast<const unsigned char*>(c->d_state),
+                                                    static_cast<unsigned char*>(c->d_lam), c->d_E, (uint32_t)n_el,
+                                                    p->objective, (int)e0, s0);
+    BK_CUDA(c, cudaGetLastError());
+  }
+  size_t ri = 0;
+  for (int j = 0; j < T; ++j) {
+    size_t e = 0;
+    BK_TRY(ev_begin(c, "adj_a1", &e));
+    adj_pass_kernel<R><<<g1, kComputeThreads, AdjSmem::kBytes, st>>>(dd, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0, err);
+    BK_CUDA(c, cudaGetLastError());
+    BK_TRY(ev_end(c, e));
+    BK_TRY(ev_begin(c, "adj_s2", &e));
+    adj_pass_kernel<R><<<g2, kComputeThreads, AdjSmem::kBytes, st>>>(dd, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1, err);
+    BK_CUDA(c, cudaGetLastError());
+    BK_TRY(ev_end(c, e));
+    if (w3 > 0) {
+      BK_TRY(ev_begin(c, "adj_s3", &e));
+      adj_pass_kernel<R><<<g3, kComputeThreads, AdjSmem::kBytes, st>>>(dd, TASK_S3, (uint32_t)j, 0, 1, err);
+      BK_CUDA(c, cudaGetLastError());
+      BK_TRY(ev_end(c, e));
+    }
+    if (ri < resets.size() && resets[ri].after_j == j) {
+      const Reset& r = resets[ri];
+      BK_TRY(ev_begin(c, "adj_reset", &e));
+      adj_reset_kernel<R><<<kResetGrid, kComputeThreads, 0, st>>>(
+          static_cast<unsigned char*>(c->d_state), ckpt + (size_t)r.ck * sbytes, c->d_E, (uint32_t)n_el, run.phase,
+          r.a, r.b, d_dev + ri * kResetGrid);
+      BK_CUDA(c, cudaGetLastError());
+      BK_TRY(ev_end(c, e));
+      ++ri;
+    }
+  }
+  BK_CUDA(c, cudaEventRecord(ev[3], st));
+  std::vector<double> cross((size_t)T), dev(std::max<size_t>(resets.size(), 1) * kResetGrid, 0.0);
+  int e_dev = 0;
+  BK_CUDA(c, cudaMemcpyAsync(cross.data(), d_cross, (size_t)T * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (!resets.empty())
+    BK_CUDA(c, cudaMemcpyAsync(dev.data(), d_dev, resets.size() * kResetGrid * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
+  BK_CUDA(c, cudaMemcpyAsync(&e_dev, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  BK_CUDA(c, cudaStreamSynchronize(st));
+  if (e_dev != 0) return fail(c, BK_ERR_TIMEOUT, "adjoint sweep: a bounded device wait gave up (%d)", e_dev);
+  BK_TRY(collect_timing(c));
+  for (int j = 0; j < T; ++j) {
+    const int k = T - 1 - j;
+    (*grad_step)[(size_t)k] =
+        (double)(-2.0L * (long double)p->dt * (long double)cross[(size_t)j] * std::exp2(-wlog2[(size_t)j]));
+  }
+  if (stats) {
+    float rv_ms = 0.f;
+    BK_CUDA(c, cudaEventElapsedTime(&rv_ms, ev[2], ev[3]));
+    stats->reverse_ms = rv_ms;
+    double mx = 0.0;
+    for (size_t r = 0; r < resets.size(); ++r) {
+      double sacc = 0.0;
+      for (int i = 0; i < kResetGrid; ++i) sacc += dev[r * kResetGrid + (size_t)i];
+      mx = std::max(mx, std::sqrt(sacc));
+    }
+    stats->max_drift = mx;
+  }
+  return BK_OK;
+}
+
 int check_device_error(bk_ctx* c) {
   int e = 0;
   BK_CUDA(c, cudaMemcpyAsync(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1381,7 +1717,8 @@ int bk_destroy(bk_ctx* c) {
                   (void*)c->d_rand, (void*)c->d_samples, (void*)c->d_binom, (void*)c->d_found})
     if (p) cudaFree(p);
   for (auto& kv : c->batch_E) cudaFree(kv.second);
-  for (void* p : {c->d_batch_state, c->d_batch, (void*)c->d_batch_results, c->d_persist})
+  for (void* p : {c->d_batch_state, c->d_batch, (void*)c->d_batch_results, c->d_persist, c->d_lam, c->d_ckpt,
+                  c->d_adj})
     if (p) cudaFree(p);
   for (auto& e : c->ev_pool) {
     cudaEventDestroy(e.first);
@@ -1625,6 +1962,70 @@ int bk_evolve(bk_ctx* c, const bk_evolve_params* p, double* p_less, double* d_h,
   }
   if (status == BK_ERR_NORM) return fail(c, BK_ERR_NORM, "norm left the tolerance band %g", p->norm_tol);
   return BK_OK;
+}
+
+int bk_adjoint(bk_ctx* c, const bk_adjoint_params* p, double* value_out, double* grad_out,
+               double* grad_steps_out, bk_adjoint_stats* stats) {
+  if (!c || !p) return BK_ERR_INVALID;
+  if (p->precision != BK_C64 && p->precision != BK_C128) return fail(c, BK_ERR_INVALID, "precision %d", p->precision);
+  const int nmin = p->precision == BK_C64 ? 14 : 13;
+  if (p->n < nmin || p->n > kMaxN)
+    return fail(c, BK_ERR_UNSUPPORTED, "adjoint: n = %d outside [%d, %d] for this precision", p->n, nmin, kMaxN);
+  if (p->n_steps < 0 || p->n_segments < 1) return fail(c, BK_ERR_INVALID, "n_steps / n_segments");
+  if (p->objective != BK_OBJ_P_LESS && p->objective != BK_OBJ_D_H)
+    return fail(c, BK_ERR_INVALID, "objective %d", p->objective);
+  if (!p->g || !grad_out) return fail(c, BK_ERR_INVALID, "g and grad_out must not be NULL");
+  if (!is_finite(p->dt) || !is_finite(p->diag_scale)) return fail(c, BK_ERR_INVALID, "dt / diag_scale not finite");
+  if (!p->segment_of_step && p->n_steps % p->n_segments != 0)
+    return fail(c, BK_ERR_INVALID, "n_steps %d is not a multiple of n_segments %d", p->n_steps, p->n_segments);
+  const int n = p->n, T = p->n_steps;
+  std::vector<int> seg((size_t)T);
+  std::vector<double> g_step((size_t)T);
+  for (int k = 0; k < T; ++k) {
+    seg[(size_t)k] = p->segment_of_step ? p->segment_of_step[k] : k / (T / p->n_segments);
+    if (seg[(size_t)k] < 0 || seg[(size_t)k] >= p->n_segments)
+      return fail(c, BK_ERR_INVALID, "segment_of_step[%d] = %d", k, seg[(size_t)k]);
+    g_step[(size_t)k] = p->g[seg[(size_t)k]];
+    if (!is_finite(g_step[(size_t)k])) return fail(c, BK_ERR_INVALID, "g of segment %d not finite", seg[(size_t)k]);
+    if (std::cos(g_step[(size_t)k] * p->dt) == 0.0) return fail(c, BK_ERR_INVALID, "cos(g dt) = 0 at step %d", k);
+  }
+  int64_t e0 = p->e0;
+  if (e0 < 0) BK_TRY(bk_labs_energy(n, &p->s0, 1, &e0));
+  const double angle_unit = (p->diag_scale > 0.0) ? p->dt * p->diag_scale : p->dt / (double)n;
+  BK_CUDA(c, cudaSetDevice(c->device));
+  BK_TRY(ensure_energy(c, n));
+  BK_TRY(ensure_state(c, n, p->precision));
+  BK_TRY(ensure_buffer(c, reinterpret_cast<void**>(&c->d_results), &c->results_cap, 4 * sizeof(double)));
+  BK_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+  const size_t sbytes = (1ull << n) * amp_bytes(p->precision);
+  // checkpoints: every K steps strictly inside (0, T); K enlarged until they fit
+  size_t free_b = 0, total_b = 0;
+  BK_CUDA(c, cudaMemGetInfo(&free_b, &total_b));
+  const size_t reserve = (size_t)1 << 30;
+  const size_t avail = free_b + c->lam_cap + c->ckpt_cap;
+  if (avail < sbytes + reserve) return fail(c, BK_ERR_OOM, "adjoint: no room for the adjoint statevector");
+  int K = p->checkpoint_every;
+  const bool auto_k = K <= 0;
+  if (auto_k) K = 128;
+  auto n_ck = [&](int k) { return T > 0 ? (T - 1) / k : 0; };
+  while (sbytes * (size_t)(1 + n_ck(K)) + reserve > avail) {
+    if (!auto_k) return fail(c, BK_ERR_OOM, "adjoint: %d checkpoints of %zu bytes do not fit", n_ck(K), sbytes);
+    K *= 2;
+  }
+  const int n_ckpt = n_ck(K);
+  BK_TRY(ensure_buffer(c, &c->d_lam, &c->lam_cap, sbytes));
+  if (n_ckpt > 0) BK_TRY(ensure_buffer(c, &c->d_ckpt, &c->ckpt_cap, sbytes * (size_t)n_ckpt));
+  c->tma.clear();
+  std::vector<double> gs;
+  if (p->precision == BK_C64)
+    BK_TRY(adjoint_t<float>(c, p, g_step, e0, angle_unit, K, n_ckpt, value_out, &gs, stats));
+  else
+    BK_TRY(adjoint_t<double>(c, p, g_step, e0, angle_unit, K, n_ckpt, value_out, &gs, stats));
+  for (int j = 0; j < p->n_segments; ++j) grad_out[j] = 0.0;
+  for (int k = 0; k < T; ++k) grad_out[seg[(size_t)k]] += gs[(size_t)k];
+  if (grad_steps_out)
+    for (int k = 0; k < T; ++k) grad_steps_out[k] = gs[(size_t)k];
+  return check_device_error(c);
 }
 
 int bk_d_min(bk_ctx* c, int n, uint64_t bits, int64_t target, int max_d, int* d_out) {

@@ -237,6 +237,50 @@ enum { BK_OPT_ENGINE_MODE = 0, BK_OPT_SLAB_LAG = 1 };
 int bk_set_option(bk_ctx* ctx, int option, int64_t value);
 int bk_get_option(const bk_ctx* ctx, int option, int64_t* value);
 
+/* ---- Adjoint gradient of a piecewise-constant field schedule ----
+ *
+ * No counterpart in the reference (whose field is constant in time); the step
+ * is the reference's psi_{k+1} = M(g_k) D psi_k (sampler.cuh:604-618) with the
+ * field g_k = g[segment_of_step[k]]. Computes O(T) = <psi_T| W |psi_T> for a
+ * diagonal W (BK_OBJ_P_LESS: [E(s) < e0], the reference's P_< of
+ * sampler.cuh:149-195; BK_OBJ_D_H: popcount(s ^ s0), its <d_H>) and dO/dg_j for
+ * every segment by one forward run and one reverse sweep of the adjoint state
+ * lambda_k = (M D)^dagger lambda_{k+1} together with psi_k rebuilt by inverse
+ * steps (no stored trajectory); psi is reset from a checkpoint every
+ * checkpoint_every steps to bound the drift of the inverse steps. */
+enum { BK_OBJ_P_LESS = 0, BK_OBJ_D_H = 1 };
+
+typedef struct bk_adjoint_params {
+  int32_t n;                      /* qubits: 14..30 (complex64) or 13..30 (complex128) */
+  int32_t precision;              /* bk_precision */
+  uint64_t s0;                    /* trap bits (initial state |s0>) */
+  int64_t e0;                     /* P_< threshold; < 0 means E(s0) */
+  double dt;
+  double diag_scale;              /* <= 0: 1/n */
+  int32_t n_steps;
+  int32_t n_segments;
+  const double* g;                /* [n_segments] field of each segment */
+  const int32_t* segment_of_step; /* [n_steps] segment of each step, or NULL: equal consecutive
+                                     segments (n_steps a multiple of n_segments) */
+  int32_t checkpoint_every;       /* K; <= 0: 128, enlarged until the checkpoints fit in free memory */
+  int32_t objective;              /* BK_OBJ_P_LESS or BK_OBJ_D_H */
+} bk_adjoint_params;
+
+typedef struct bk_adjoint_stats {
+  double value;                   /* O(T) */
+  double norm;                    /* |psi_T|^2 */
+  int32_t checkpoint_every;       /* K used */
+  int32_t n_checkpoints;
+  double max_drift;               /* max over checkpoints of |psi_rebuilt - psi_k| (2-norm) */
+  double forward_ms;              /* device time of the forward run (with checkpoint copies) */
+  double reverse_ms;              /* device time of the reverse sweep */
+} bk_adjoint_stats;
+
+/* grad_out[n_segments] = dO/dg_j; grad_steps_out (NULL or [n_steps]) = dO/dg_k per
+ * step; value_out and stats may be NULL. */
+int bk_adjoint(bk_ctx* ctx, const bk_adjoint_params* p, double* value_out, double* grad_out,
+               double* grad_steps_out, bk_adjoint_stats* stats);
+
 /* ---- Projective sampling (sampler.cuh:459-487, 559-598) ---- */
 
 /* Samples `shots` basis states from |psi|^2 of the state left by the last
