@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--workload", choices=["large", "batched"], default="large",
                     help="large: the N=28 headline; batched: 512 instances (64 traps x 8 g), N in {16,18,20,22}")
     ap.add_argument("--slab-lag", type=int, default=None)
+    ap.add_argument("--split-w2", type=int, default=None, help="qubits of the S2 pass (0 = default split)")
+    ap.add_argument("--no-tune", action="store_true", help="engine defaults instead of the autotuner's choice")
     return ap.parse_args()
 
 
@@ -175,6 +177,23 @@ def run_reference(a):
     print(json.dumps(line))
 
 
+def tuned_knobs(eng, a, n, prec, trap):
+    """Engine knobs for this run: explicit flags, else the autotuner's cached choice
+    for this device and size, else a tuning sweep now (not timed, not cached)."""
+    from bk_b200 import tune
+    explicit = {k: v for k, v in (("engine_mode", a.engine_mode), ("slab_lag", a.slab_lag),
+                                  ("split_w2", a.split_w2)) if v is not None}
+    if explicit or a.no_tune:
+        for k, v in explicit.items():
+            eng.set_option(k, v)
+        return dict(source="flags" if explicit else "engine defaults", **explicit)
+    best = tune.apply(eng, n, prec)
+    if best is not None:
+        return dict(source="autotuner cache (bk_b200/tuning/b200.json)", **best)
+    entry = tune.tune(eng, n, prec, steps=10, warmup=2, trap=trap, write=False)
+    return dict(source="autotuner sweep at start-up (untimed)", **entry["best"])
+
+
 def batched_instances(seed=2024):
     """64 traps (seeded descents, lowest 5% of 1000) with N drawn from {16,18,20,22}, x 8 g in [0.2, 0.5]."""
     import bk_b200 as bk
@@ -197,15 +216,22 @@ def run_batched(a):
     amp_steps = float(sum(1 << d["n"] for d in inst)) * steps_t
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=dev)
     meas = range(0, steps_t + 1)
+    from bk_b200 import tune
+    lag = tune.batch_lag(eng, inst)
+    lag_src = "autotuner cache (bk_b200/tuning/b200.json)"
+    if lag is None:
+        lag = tune.tune_batch(eng, inst, a.dt, steps_t, measure=meas, write=False)["best"]["lag"]
+        lag_src = "autotuner sweep at start-up (untimed)"
     for _ in range(max(a.warmup, 1)):
-        eng.evolve_batch(inst, a.dt, steps_t, measure=meas, precision=bk.BK_C64, use_graph=True)
+        eng.evolve_batch(inst, a.dt, steps_t, measure=meas, precision=bk.BK_C64, use_graph=True, lag=lag)
     torch.cuda.synchronize(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clocks:
         t0 = time.perf_counter()
         ev0.record(stream)
         for _ in range(a.steps):
-            p, d, nn = eng.evolve_batch(inst, a.dt, steps_t, measure=meas, precision=bk.BK_C64, use_graph=True)
+            p, d, nn = eng.evolve_batch(inst, a.dt, steps_t, measure=meas, precision=bk.BK_C64, use_graph=True,
+                                        lag=lag)
         ev1.record(stream)
         torch.cuda.synchronize(dev)
         wall = time.perf_counter() - t0
@@ -236,6 +262,7 @@ def run_batched(a):
                                    "steps, P_< and <d_H> every step; one persistent launch through a captured "
                                    "CUDA graph per bench step",
                        "instances": len(inst), "trotter_steps_per_step": steps_t,
+                       "tuning": {"lag": lag, "source": lag_src},
                        "amp_steps_per_step": amp_steps},
             "compare": dict(seq, batched_over_best_sequential=value / best_seq),
             "e2e": {"value": amp_steps * a.steps / wall, "unit": UNIT, "h2d_bytes_per_step": 24 * len(inst) + 501,
@@ -280,11 +307,8 @@ def main():
     n, T = a.n, a.trotter
     prec = bk.BK_C64 if a.precision == "c64" else bk.BK_C128
     eng = bk.Engine(local)
-    if a.engine_mode is not None:
-        eng.set_option("engine_mode", a.engine_mode)
-    if a.slab_lag is not None:
-        eng.set_option("slab_lag", a.slab_lag)
     bits, e0 = bk.select_trap(n, 42 + rank, 4000, 0.01)
+    tuning = tuned_knobs(eng, a, n, prec, (bits, e0))
     meas = list(range(0, T + 1, a.measure_every))
     dev = torch.device("cuda", local)
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=dev)
@@ -352,7 +376,7 @@ def main():
                                    f"{a.measure_every} steps, {a.precision} fused",
                        "n": n, "trap_bits": hex(bits), "trap_energy": e0, "trotter_steps_per_step": T,
                        "l2": f"state {((1 << n) * S) / 2**30:.1f} GiB > 126 MB L2, no flush needed",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", "tuning": tuning},
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": dms / dl,

@@ -196,6 +196,7 @@ class Engine:
 
     def __init__(self, device=0):
         self.L = load_library()
+        self.device = device
         self.ctx = ctypes.c_void_p()
         st = self.L.bk_create(device, ctypes.byref(self.ctx))
         if st != BK_OK:
@@ -369,7 +370,7 @@ class Engine:
         self._check(self.L.bk_sample(self.ctx, _p(r, _dp), len(r), _p(out, _u64p)), "bk_sample")
         return out
 
-    OPTIONS = {"engine_mode": 0, "slab_lag": 1}
+    OPTIONS = {"engine_mode": 0, "slab_lag": 1, "split_w2": 2}
 
     def set_option(self, name, value):
         self._check(self.L.bk_set_option(self.ctx, self.OPTIONS[name], int(value)), "bk_set_option")

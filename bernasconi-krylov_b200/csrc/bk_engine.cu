@@ -89,6 +89,7 @@ struct bk_ctx {
   bool planar = false;        // complex64 state stored pair-planar (persistent engine)
   int slab_lag = 3;           // persistent engine: S2 queue lag behind A1, in slabs
   int engine_mode = 0;        // 0 persistent dataflow, 1 one launch per pass (tile grid)
+  int force_w2 = 0;           // S2 width when > 0 and valid for the size (else the default split)
   std::map<int, uint16_t*> batch_E;  // E tables of batched runs, per n
   void* d_batch_state = nullptr;
   size_t batch_state_cap = 0;
@@ -612,6 +613,15 @@ struct PersistRun {
   typename PhaseV<R>::params phase{};  // device tables of the diagonal phase
 };
 
+// Width of the S2 pass for `rest` element bits above the A1 tile: the engine's
+// default (everything in S2 up to 9 bits, else an even split), or the forced
+// width when it leaves at most 9 bits for S3.
+int split_w2(const bk_ctx* c, int rest) {
+  const int w = c->force_w2;
+  if (w >= 1 && w <= 9 && w <= rest && rest - w <= 9) return w;
+  return (rest <= 9) ? rest : (rest + 1) / 2;
+}
+
 template <class R>
 int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double angle_unit,
                     const std::vector<R>& tans, const std::vector<R>& scales, PersistRun<R>* run) {
@@ -620,7 +630,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   const int np = c64 ? n - 1 : n;  // element bits
   const int rest = np - kElemBits;
   if (rest < 1) return fail(c, BK_ERR_UNSUPPORTED, "persistent engine needs n > %d", kElemBits + (c64 ? 1 : 0));
-  const int w2 = (rest <= 9) ? rest : (rest + 1) / 2;
+  const int w2 = split_w2(c, rest);
   const int w3 = rest - w2;
   if (w2 > 9 || w3 > 9) return fail(c, BK_ERR_UNSUPPORTED, "n = %d needs more than two strided passes", n);
   const int e_tile_bits = c64 ? 13 : 12;
@@ -944,7 +954,7 @@ int evolve_batch_t(bk_ctx* c, const bk_batch_params* bp, const bk_batch_instance
       return fail(c, BK_ERR_UNSUPPORTED, "batched instance %d: n = %d outside [%d, %d]", i, b.n,
                   kElemBits + (c64 ? 2 : 1), kMaxN);
     const int rest = g.np - kElemBits;
-    g.w2 = (rest <= 9) ? rest : (rest + 1) / 2;
+    g.w2 = split_w2(c, rest);
     g.w3 = rest - g.w2;
     if (g.w2 > 9 || g.w3 > 9) return fail(c, BK_ERR_UNSUPPORTED, "n = %d needs more than two strided passes", b.n);
     g.n_a1 = 1u << (g.np - kElemBits);
@@ -1817,6 +1827,10 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
       if (value < 1 || value > 64) return fail(c, BK_ERR_INVALID, "slab lag %lld", (long long)value);
       c->slab_lag = (int)value;
       return BK_OK;
+    case BK_OPT_SPLIT_W2:
+      if (value < 0 || value > 9) return fail(c, BK_ERR_INVALID, "S2 width %lld", (long long)value);
+      c->force_w2 = (int)value;
+      return BK_OK;
     default:
       return fail(c, BK_ERR_INVALID, "unknown option %d", option);
   }
@@ -1827,6 +1841,7 @@ int bk_get_option(const bk_ctx* c, int option, int64_t* value) {
   switch (option) {
     case BK_OPT_ENGINE_MODE: *value = c->engine_mode; return BK_OK;
     case BK_OPT_SLAB_LAG: *value = c->slab_lag; return BK_OK;
+    case BK_OPT_SPLIT_W2: *value = c->force_w2; return BK_OK;
     default: return BK_ERR_INVALID;
   }
 }

@@ -45,3 +45,29 @@ def test_grid_mode_matches_oracle_c128(eng):
     assert np.max(np.abs(p - po)) <= 1e-10
     assert np.max(np.abs(d - do)) <= 1e-10 * n
     assert np.max(np.abs(nn - 1.0)) <= 1e-10
+
+
+@pytest.mark.parametrize("w2", [4, 6])
+def test_forced_split_matches_oracle_c128(eng, w2):
+    """S2 width forced by the tuner's knob (the rest goes to S3): same physics."""
+    n, steps = 22, 16
+    bits, e0 = bk.select_trap(n, 8, 200, 0.05)
+    eng.set_option("split_w2", w2)
+    p, d, nn = eng.evolve(n, bits, 0.35, 0.05, steps, e0=e0, precision=bk.BK_C128)
+    eng.set_option("split_w2", 0)
+    po, do, _ = O.trotter_evolve(n, bits, e0, 0.35, 0.05, steps)
+    assert np.max(np.abs(p - po)) <= 1e-10
+    assert np.max(np.abs(d - do)) <= 1e-10 * n
+
+
+def test_tuner_sweeps_and_caches(eng, tmp_path):
+    from bk_b200 import tune
+    path = str(tmp_path / "cache.json")
+    e = tune.tune(eng, 20, bk.BK_C64, steps=4, warmup=1, cache_path=path)
+    assert len(e["candidates"]) == len(tune.candidates(20, bk.BK_C64))
+    assert e["amp_steps_per_s"] == max(c["amp_steps_per_s"] for c in e["candidates"])
+    eng.set_option("engine_mode", 0)
+    assert tune.apply(eng, 20, bk.BK_C64, cache_path=path) == e["best"]
+    assert eng.get_option("engine_mode") == e["best"]["engine_mode"]
+    for k in tune.KNOBS:
+        eng.set_option(k, {"engine_mode": 0, "slab_lag": 3, "split_w2": 0}[k])
