@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
     ap.add_argument("--engine-mode", type=int, default=None, help="0 persistent, 1 one launch per pass")
-    ap.add_argument("--workload", choices=["large", "batched"], default="large",
+    ap.add_argument("--workload", choices=["large", "batched", "adjoint"], default="large",
                     help="large: the N=28 headline; batched: 512 instances (64 traps x 8 g), N in {16,18,20,22}")
     ap.add_argument("--slab-lag", type=int, default=None)
     ap.add_argument("--split-w2", type=int, default=None, help="qubits of the S2 pass (0 = default split)")
@@ -273,6 +273,63 @@ def run_batched(a):
     print(json.dumps(line))
 
 
+def run_adjoint(a):
+    """Adjoint gradient: N=22 trap (lowest 5% of 1000 descents), 64 segments g_j ~ U[0.25, 0.45], dt=0.02,
+    1280 steps, checkpoints every 128; one bench step = one bk_adjoint call (value and 64 gradients)."""
+    import torch
+    import bk_b200 as bk
+    n, nseg, T, K = 22, 64, 1280, 128
+    prec = bk.BK_C64 if a.precision == "c64" else bk.BK_C128
+    dev = torch.device("cuda", 0)
+    eng = bk.Engine(0)
+    bits, e0 = bk.select_trap(n, 42, 1000, 0.05)
+    gs = np.random.default_rng(42).uniform(0.25, 0.45, nseg)
+    g_steps = np.repeat(gs, T // nseg)
+    stream = torch.cuda.ExternalStream(eng.stream_handle(), device=dev)
+    for _ in range(max(a.warmup, 1)):
+        eng.adjoint(n, bits, gs, a.dt, T, e0=e0, precision=prec, checkpoint_every=K)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fw, rv = [], []
+    with ClockSampler(0) as clocks:
+        t0 = time.perf_counter()
+        ev0.record(stream)
+        for _ in range(a.steps):
+            val, grad, st = eng.adjoint(n, bits, gs, a.dt, T, e0=e0, precision=prec, checkpoint_every=K)
+            fw.append(st["forward_ms"])
+            rv.append(st["reverse_ms"])
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - t0
+    dev_s = ev0.elapsed_time(ev1) / 1e3
+    # one plain forward run of the same schedule (measurement at T only)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(a.steps):
+        eng.evolve(n, bits, g_steps, a.dt, T, measure=[T], e0=e0, precision=prec)
+    f1.record(stream)
+    torch.cuda.synchronize(dev)
+    fwd_s = f0.elapsed_time(f1) / 1e3 / a.steps
+    amp_steps = float(1 << n) * T
+    line = {"metric": "Adjoint gradient amp-steps/s (N=22, 64 segments, 1280 steps; forward + reverse sweep)",
+            "value": amp_steps * a.steps / dev_s, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * dev_s / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": a.precision, "data": "synthetic (seeded trap and field schedule, no dataset)",
+            "config": {"workload": "N=22 trap (lowest 5% of 1000 descents, seed 42), 64 segments g_j ~ U[0.25, 0.45] "
+                                   "(seed 42), dt=0.02, 1280 steps, checkpoints every 128, objective P_<(T)",
+                       "n": n, "segments": nseg, "trotter_steps": T, "checkpoint_every": K,
+                       "l2": "two 32 MiB statevectors (complex64) fit the 126 MB L2"},
+            "compare": {"forward_ms": 1e3 * fwd_s, "gradient_ms": 1e3 * dev_s / a.steps,
+                        "gradient_cost_in_forwards": dev_s / a.steps / fwd_s,
+                        "reverse_over_forward": float(np.mean(rv)) / float(np.mean(fw)),
+                        "max_checkpoint_drift": st["max_drift"]},
+            "e2e": {"value": amp_steps * a.steps / wall, "unit": UNIT, "h2d_bytes_per_step": 8 * nseg + 96,
+                    "d2h_bytes_per_step": 8 * (nseg + 1 + T)},
+            "clocks": clocks.summary(), "check": {"p_less_T": val, "grad_max_abs": float(np.max(np.abs(grad)))}}
+    eng.close()
+    print(json.dumps(line))
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -280,6 +337,9 @@ def main():
         return
     if a.workload == "batched":
         run_batched(a)
+        return
+    if a.workload == "adjoint":
+        run_adjoint(a)
         return
     import torch
     import torch.distributed as dist

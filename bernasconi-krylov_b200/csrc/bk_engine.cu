@@ -298,23 +298,6 @@ int build_e_map(bk_ctx* c, const uint16_t* E, int n, int T, TmaDesc* out) {
   return BK_OK;
 }
 
-int get_map(bk_ctx* c, const std::string& kind, int n, int prec, int cp, int h0, int w, const TmaDesc** out) {
-  char key[160];
-  snprintf(key, sizeof(key), "%s/%p/%p/%d/%d/%d/%d/%d", kind.c_str(), c->d_state, (void*)c->d_E, n, prec, cp,
-           h0, w);
-  auto it = c->tma.find(key);
-  if (it == c->tma.end()) {
-    TmaDesc d;
-    if (kind == "E")
-      BK_TRY(build_e_map(c, c->d_E, n, tile_bits(prec), &d));
-    else
-      BK_TRY(build_amp_map(c, c->d_state, n, prec, cp, h0, w, &d));
-    it = c->tma.emplace(key, d).first;
-  }
-  *out = &it->second;
-  return BK_OK;
-}
-
 int ensure_energy(bk_ctx* c, int n) {
   if (c->e_n == n && c->d_E) return BK_OK;
   if (c->d_E) cudaFree(c->d_E);
@@ -502,56 +485,6 @@ template <class A>
 int launch_sampling(bk_ctx* c, const A* psi, int n, int pt, int shots) {
   if (c->planar) return launch_sampling_t(c, reinterpret_cast<const Planar64*>(psi), n, pt, shots);
   return launch_sampling_t(c, psi, n, pt, shots);
-}
-
-template <class R>
-int launch_a1(bk_ctx* c, int kind, const PassParams<R>& pp, const TmaDesc* am, const TmaDesc* em, int n) {
-  constexpr int T = AmpTraits<R>::kTileBits;
-  const unsigned grid = 1u << (n - T);
-  const int smem = SmemLayout<R>::kA1Bytes;
-  size_t ev = 0;
-  if (kind == 0) {
-    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(a1_kernel<R, 0>), smem));
-    BK_TRY(ev_begin(c, pp.measure ? "a1_step_measure" : "a1_step", &ev));
-    a1_kernel<R, 0><<<grid, kThreads, smem, c->stream>>>(am->map, em->map, pp);
-  } else {
-    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(a1_kernel<R, 1>), smem));
-    BK_TRY(ev_begin(c, "a1_measure", &ev));
-    a1_kernel<R, 1><<<grid, kThreads, smem, c->stream>>>(am->map, em->map, pp);
-  }
-  BK_CUDA(c, cudaGetLastError());
-  return ev_end(c, ev);
-}
-
-template <class R, int W>
-int launch_strided_w(bk_ctx* c, const PassParams<R>& pp, const TmaDesc* am, int n) {
-  constexpr int T = AmpTraits<R>::kTileBits;
-  const unsigned grid = 1u << (n - T);
-  const int smem = SmemLayout<R>::kStridedBytes;
-  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(strided_kernel<R, W>), smem));
-  size_t ev = 0;
-  char name[32];
-  snprintf(name, sizeof(name), "strided_w%d", W);
-  BK_TRY(ev_begin(c, name, &ev));
-  strided_kernel<R, W><<<grid, kThreads, smem, c->stream>>>(am->map, pp);
-  BK_CUDA(c, cudaGetLastError());
-  return ev_end(c, ev);
-}
-
-template <class R>
-int launch_strided(bk_ctx* c, int w, const PassParams<R>& pp, const TmaDesc* am, int n) {
-  switch (w) {
-    case 1: return launch_strided_w<R, 1>(c, pp, am, n);
-    case 2: return launch_strided_w<R, 2>(c, pp, am, n);
-    case 3: return launch_strided_w<R, 3>(c, pp, am, n);
-    case 4: return launch_strided_w<R, 4>(c, pp, am, n);
-    case 5: return launch_strided_w<R, 5>(c, pp, am, n);
-    case 6: return launch_strided_w<R, 6>(c, pp, am, n);
-    case 7: return launch_strided_w<R, 7>(c, pp, am, n);
-    case 8: return launch_strided_w<R, 8>(c, pp, am, n);
-    case 9: return launch_strided_w<R, 9>(c, pp, am, n);
-    default: return fail(c, BK_ERR_UNSUPPORTED, "strided pass width %d", w);
-  }
 }
 
 // ---------------------------------------------------------------------------
