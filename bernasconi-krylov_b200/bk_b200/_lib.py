@@ -61,6 +61,17 @@ class AdjointStatsC(ctypes.Structure):
                 ("reverse_ms", ctypes.c_double)]
 
 
+class MinimumFamilyC(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("canonical_state", ctypes.c_uint64), ("sample_state", ctypes.c_uint64),
+                ("energy", ctypes.c_int64), ("times_visited", ctypes.c_uint64),
+                ("evals_to_first_find", ctypes.c_uint64)]
+
+
+class CollectStatsC(ctypes.Structure):
+    _fields_ = [("total_starts", ctypes.c_uint64), ("total_evals", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("saturated", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
 class SamplerConfigC(ctypes.Structure):
     """bk_sampler_config — the reference's SamplerConfig (sampler.cuh:235-260) plus precision/method."""
     _fields_ = [("n", ctypes.c_int32), ("num_sample_points", ctypes.c_int32), ("shots_per_point", ctypes.c_int32),
@@ -130,6 +141,11 @@ def load_library(build_if_missing=True):
     L.bk_evolve_batch.argtypes = [c_ctx, ctypes.POINTER(BatchParamsC), ctypes.POINTER(BatchInstanceC), ctypes.c_int32,
                                   _dp, _dp, _dp]
     L.bk_get_option.argtypes = [c_ctx, ctypes.c_int, _i64p]
+    L.bk_steepest_descent_gpu.argtypes = [c_ctx, ctypes.c_int, _u64p, ctypes.c_int64, ctypes.c_uint64, _u64p, _i64p,
+                                          _u64p]
+    L.bk_collect_minima.argtypes = [c_ctx, ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64,
+                                    ctypes.c_int64, ctypes.POINTER(MinimumFamilyC), ctypes.c_int64, _i64p,
+                                    ctypes.POINTER(CollectStatsC)]
     L.bk_adjoint.argtypes = [c_ctx, ctypes.POINTER(AdjointParamsC), _dp, _dp, _dp, ctypes.POINTER(AdjointStatsC)]
     L.bk_sampler_run.argtypes = [c_ctx, ctypes.POINTER(SamplerConfigC), ctypes.c_uint64,
                                  ctypes.POINTER(SamplingResultC)]
@@ -320,6 +336,28 @@ class Engine:
         if per_step:
             stats["grad_steps"] = gsteps[:n_steps]
         return float(val[0]), grad, stats
+
+    def steepest_descent(self, n, starts, max_evals=0):
+        """Device batched descent (bit-exact with the module-level host version):
+        (final_states, final_energies, evals)."""
+        st = np.ascontiguousarray(starts, dtype=np.uint64)
+        fs = np.empty(len(st), dtype=np.uint64)
+        fe = np.empty(len(st), dtype=np.int64)
+        ev = np.empty(len(st), dtype=np.uint64)
+        self._check(self.L.bk_steepest_descent_gpu(self.ctx, n, _p(st, _u64p), len(st), max_evals, _p(fs, _u64p),
+                                                   _p(fe, _i64p), _p(ev, _u64p)), "bk_steepest_descent_gpu")
+        return fs, fe, ev
+
+    def collect_minima(self, n, seed=42, target_families=100, batch_size=4096, max_starts=100000):
+        """Distinct local-minimum families (list of dicts, deepest first) and run statistics."""
+        cap = int(target_families)
+        arr = (MinimumFamilyC * cap)()
+        cnt = ctypes.c_int64()
+        st = CollectStatsC()
+        self._check(self.L.bk_collect_minima(self.ctx, n, seed, target_families, batch_size, max_starts, arr, cap,
+                                             ctypes.byref(cnt), ctypes.byref(st)), "bk_collect_minima")
+        fams = [{k: getattr(arr[i], k) for k, _ in MinimumFamilyC._fields_} for i in range(min(cnt.value, cap))]
+        return fams, {k: getattr(st, k) for k, _ in CollectStatsC._fields_}
 
     def d_min(self, n, bits, target=-1, max_d=-1):
         d = ctypes.c_int()

@@ -374,4 +374,86 @@ __global__ void dmin_sphere_kernel(int n, uint32_t s, int target, int d, unsigne
   }
 }
 
+// ---------------------------------------------------------------------------
+// Batched single-flip steepest descent (reference: batch_steepest_descent_kernel,
+// src/classical/classical.cuh:459-540; CPU form :625-712). One warp per start:
+// lane l scores the flips p = l, l + 32 from the shared autocorrelations C_k
+// (C_k + d_k(p))^2 summed over k, the warp keeps the lowest energy and, among
+// equal energies, the lowest p — the flip the sequential scan (first strictly
+// better) takes; lanes own C_k for k = l, l + 32 for the update. An iteration
+// costs n evaluations and runs only while evals + n <= budget, as in the reference.
+// ---------------------------------------------------------------------------
+constexpr int kDescentWarps = 8;
+
+__device__ __forceinline__ int spin_of(uint64_t x, int i) { return ((x >> i) & 1ull) ? -1 : 1; }
+
+__global__ void __launch_bounds__(32 * kDescentWarps)
+    descent_kernel(int n, const uint64_t* __restrict__ starts, long long count, unsigned long long budget,
+                   uint64_t* __restrict__ final_states, long long* __restrict__ final_energies,
+                   unsigned long long* __restrict__ evals_out) {
+  __shared__ int Cs[kDescentWarps][64];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const long long i = (long long)blockIdx.x * kDescentWarps + wib;
+  if (i >= count) return;  // the whole warp leaves together
+  int* C = Cs[wib];
+  const uint64_t mask = (1ull << n) - 1ull;
+  uint64_t x = starts[i] & mask;
+  int part = 0;
+  for (int k = 1 + lane; k < n; k += 32) {
+    const int c = (n - k) - 2 * __popcll((x ^ (x >> k)) & ((1ull << (n - k)) - 1ull));
+    C[k] = c;
+    part += c * c;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  int e = part;
+  __syncwarp();
+  unsigned long long evals = 1;
+  while (evals + (unsigned long long)n <= budget) {
+    int best_e = e, best_p = 0x7fffffff;
+    for (int p = lane; p < n; p += 32) {
+      const int sp = spin_of(x, p);
+      int ne = 0;
+      for (int k = 1; k < n; ++k) {
+        int d = 0;
+        if (p + k < n) d -= 2 * sp * spin_of(x, p + k);
+        if (p - k >= 0) d -= 2 * sp * spin_of(x, p - k);
+        const int c = C[k] + d;
+        ne += c * c;
+      }
+      if (ne < best_e) {
+        best_e = ne;
+        best_p = p;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const int oe = __shfl_xor_sync(0xffffffffu, best_e, o);
+      const int op = __shfl_xor_sync(0xffffffffu, best_p, o);
+      if (oe < best_e || (oe == best_e && op < best_p)) {
+        best_e = oe;
+        best_p = op;
+      }
+    }
+    evals += (unsigned long long)n;
+    if (best_p == 0x7fffffff) break;  // no strictly better neighbour: a local minimum
+    const int sp = spin_of(x, best_p);
+    __syncwarp();
+    for (int k = 1 + lane; k < n; k += 32) {
+      int d = 0;
+      if (best_p + k < n) d -= 2 * sp * spin_of(x, best_p + k);
+      if (best_p - k >= 0) d -= 2 * sp * spin_of(x, best_p - k);
+      C[k] += d;
+    }
+    __syncwarp();
+    x ^= 1ull << best_p;
+    e = best_e;
+  }
+  if (lane == 0) {
+    final_states[i] = x;
+    final_energies[i] = e;
+    if (evals_out) evals_out[i] = evals;
+  }
+}
+
 }  // namespace bk

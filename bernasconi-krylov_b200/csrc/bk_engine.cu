@@ -17,6 +17,7 @@
 #include <random>
 #include <string>
 #include <unordered_set>
+#include <unordered_map>
 #include <vector>
 
 #include "bk_adjoint.cuh"
@@ -103,6 +104,8 @@ struct bk_ctx {
   size_t ckpt_cap = 0;
   void* d_adj = nullptr;      // adjoint: maps, descriptor, per-step arrays, partials
   size_t adj_cap = 0;
+  void* d_descent = nullptr;  // batched steepest descent: starts, final states, energies, evaluations
+  size_t descent_cap = 0;
   // tensor maps, keyed by (state ptr, n, precision, pass)
   std::map<std::string, TmaDesc> tma;
   // last evolution (for export / sampling)
@@ -401,6 +404,24 @@ static int64_t host_energy(int n, uint64_t x) {
     e += ck * ck;
   }
   return e;
+}
+
+// Canonical representative of the LABS symmetry orbit of s (reference:
+// SpinState::canonical, labs_energy.hpp:40-106): the smallest of s, its
+// alternating-sign image, their bit reversals, and the complements of all four.
+static uint64_t host_canonical(int n, uint64_t s) {
+  const uint64_t m = (1ull << n) - 1ull;
+  const uint64_t alt = 0x5555555555555555ull & m;
+  auto rev = [n](uint64_t x) {
+    uint64_t r = 0;
+    for (int i = 0; i < n; ++i) r |= ((x >> i) & 1ull) << (n - 1 - i);
+    return r;
+  };
+  const uint64_t a = s & m, b = a ^ alt;
+  const uint64_t cand[4] = {a, b, rev(a), rev(b)};
+  uint64_t best = ~0ull;
+  for (uint64_t c : cand) best = std::min(best, std::min(c, (~c) & m));
+  return best;
 }
 
 // Optimal LABS energies E*(n) for n <= 32 (reference: labs_energy.hpp:156-168).
@@ -1661,7 +1682,7 @@ int bk_destroy(bk_ctx* c) {
     if (p) cudaFree(p);
   for (auto& kv : c->batch_E) cudaFree(kv.second);
   for (void* p : {c->d_batch_state, c->d_batch, (void*)c->d_batch_results, c->d_persist, c->d_lam, c->d_ckpt,
-                  c->d_adj})
+                  c->d_adj, c->d_descent})
     if (p) cudaFree(p);
   for (auto& e : c->ev_pool) {
     cudaEventDestroy(e.first);
@@ -1693,6 +1714,112 @@ int bk_steepest_descent(int n, const uint64_t* starts, int64_t count, uint64_t m
   const uint64_t m = (1ull << n) - 1ull;
 #pragma omp parallel for schedule(dynamic, 16)
   for (int64_t i = 0; i < count; ++i) descend(n, starts[i] & m, max_evals, &fs[i], &fe[i], ev ? &ev[i] : nullptr);
+  return BK_OK;
+}
+
+int bk_steepest_descent_gpu(bk_ctx* c, int n, const uint64_t* starts, int64_t count, uint64_t max_evals,
+                            uint64_t* fs, int64_t* fe, uint64_t* ev) {
+  if (!c) return BK_ERR_INVALID;
+  if (n < 2 || n > 63 || count < 0 || (count > 0 && (!starts || !fs || !fe)))
+    return fail(c, BK_ERR_INVALID, "steepest descent: n = %d, count = %lld", n, (long long)count);
+  if (count == 0) return BK_OK;
+  BK_CUDA(c, cudaSetDevice(c->device));
+  const size_t cnt = (size_t)count;
+  BK_TRY(ensure_buffer(c, &c->d_descent, &c->descent_cap, cnt * 32));
+  uint64_t* d_start = static_cast<uint64_t*>(c->d_descent);
+  uint64_t* d_fs = d_start + cnt;
+  long long* d_fe = reinterpret_cast<long long*>(d_fs + cnt);
+  unsigned long long* d_ev = reinterpret_cast<unsigned long long*>(d_fe + cnt);
+  cudaStream_t st = c->stream;
+  BK_CUDA(c, cudaMemcpyAsync(d_start, starts, cnt * 8, cudaMemcpyHostToDevice, st));
+  size_t e = 0;
+  BK_TRY(ev_begin(c, "descent", &e));
+  const unsigned grid = (unsigned)((cnt + kDescentWarps - 1) / kDescentWarps);
+  descent_kernel<<<grid, 32 * kDescentWarps, 0, st>>>(n, d_start, (long long)count,
+                                                      max_evals == 0 ? ~0ull : (unsigned long long)max_evals, d_fs,
+                                                      d_fe, d_ev);
+  BK_CUDA(c, cudaGetLastError());
+  BK_TRY(ev_end(c, e));
+  BK_CUDA(c, cudaMemcpyAsync(fs, d_fs, cnt * 8, cudaMemcpyDeviceToHost, st));
+  BK_CUDA(c, cudaMemcpyAsync(fe, d_fe, cnt * 8, cudaMemcpyDeviceToHost, st));
+  if (ev) BK_CUDA(c, cudaMemcpyAsync(ev, d_ev, cnt * 8, cudaMemcpyDeviceToHost, st));
+  BK_CUDA(c, cudaStreamSynchronize(st));
+  BK_TRY(collect_timing(c));
+  return BK_OK;
+}
+
+int bk_collect_minima(bk_ctx* c, int n, uint64_t seed, int64_t target_families, int64_t batch_size,
+                      int64_t max_starts, bk_minimum_family* out, int64_t capacity, int64_t* n_out,
+                      bk_collect_stats* stats) {
+  if (!c || !n_out) return BK_ERR_INVALID;
+  if (n < 3 || n > 63 || target_families < 1 || batch_size < 1 || max_starts < 1 || capacity < 0 ||
+      (capacity > 0 && !out))
+    return fail(c, BK_ERR_INVALID, "collect_minima: bad arguments");
+  std::mt19937_64 rng(seed);
+  const uint64_t m = (1ull << n) - 1ull;
+  struct Fam {
+    bk_minimum_family f;
+    size_t order;
+  };
+  std::unordered_map<uint64_t, size_t> index;  // canonical state -> position in fams
+  std::vector<Fam> fams;
+  std::vector<uint64_t> st((size_t)batch_size), fs((size_t)batch_size), ev((size_t)batch_size);
+  std::vector<int64_t> fe((size_t)batch_size);
+  uint64_t total_evals = 0, total_starts = 0, batches = 0;
+  int stagnant = 0;
+  bool saturated = false;
+  while ((int64_t)fams.size() < target_families && total_starts < (uint64_t)max_starts) {
+    ++batches;
+    for (auto& x : st) x = rng() & m;
+    BK_TRY(bk_steepest_descent_gpu(c, n, st.data(), batch_size, 0, fs.data(), fe.data(), ev.data()));
+    total_starts += (uint64_t)batch_size;
+    size_t fresh = 0;
+    for (size_t i = 0; i < (size_t)batch_size; ++i) {
+      total_evals += ev[i];
+      const uint64_t canon = host_canonical(n, fs[i]);
+      auto it = index.find(canon);
+      if (it == index.end()) {
+        Fam f{};
+        f.f.id = fams.size() + 1;
+        f.f.canonical_state = canon;
+        f.f.sample_state = fs[i];
+        f.f.energy = fe[i];
+        f.f.times_visited = 1;
+        f.f.evals_to_first_find = total_evals;
+        f.order = fams.size();
+        index.emplace(canon, fams.size());
+        fams.push_back(f);
+        ++fresh;
+        if ((int64_t)fams.size() >= target_families) break;
+      } else {
+        fams[it->second].f.times_visited++;
+      }
+    }
+    if (fresh == 0) {
+      if (++stagnant >= 4) {
+        saturated = true;
+        break;
+      }
+    } else {
+      stagnant = 0;
+    }
+  }
+  // deepest traps first, then the most visited; discovery order breaks the remaining ties
+  std::stable_sort(fams.begin(), fams.end(), [](const Fam& a, const Fam& b) {
+    if (a.f.energy != b.f.energy) return a.f.energy < b.f.energy;
+    return a.f.times_visited > b.f.times_visited;
+  });
+  *n_out = (int64_t)fams.size();
+  for (size_t i = 0; i < fams.size() && (int64_t)i < capacity; ++i) {
+    out[i] = fams[i].f;
+    out[i].id = i + 1;
+  }
+  if (stats) {
+    stats->total_starts = total_starts;
+    stats->total_evals = total_evals;
+    stats->batches = batches;
+    stats->saturated = saturated ? 1 : 0;
+  }
   return BK_OK;
 }
 

@@ -84,6 +84,41 @@ int bk_steepest_descent(int n, const uint64_t* starts, int64_t count, uint64_t m
 int bk_select_trap(int n, uint64_t seed, int32_t n_descents, double quantile, uint64_t* trap_bits,
                    int64_t* trap_energy);
 
+/* Device form of bk_steepest_descent, bit-exact with it (replaces
+ * ClassicalOptimizer::run_batch_gpu, classical.cuh:719-770, and its
+ * batch_steepest_descent_kernel, :459-540): one warp per start. */
+int bk_steepest_descent_gpu(bk_ctx* ctx, int n, const uint64_t* starts, int64_t count, uint64_t max_evals,
+                            uint64_t* final_states, int64_t* final_energies, uint64_t* evals_out);
+
+/* Distinct local-minimum families (replaces collect_distinct_minima_gpu,
+ * classical.cuh:861-959): batches of batch_size starts from mt19937_64(seed) & mask
+ * (one stream across batches), descended on the device (unlimited evaluations);
+ * families keyed by the canonical orbit representative, first sample kept, visits
+ * counted, evaluations until first find recorded; stops at target_families, at
+ * max_starts, or after 4 batches without a new family (saturated). Output sorted
+ * by energy, then visits (descending), then discovery order; ids 1..n_out.
+ * At most `capacity` families are written; *n_out is the number found. */
+typedef struct bk_minimum_family {
+  uint64_t id;
+  uint64_t canonical_state;
+  uint64_t sample_state;
+  int64_t energy;
+  uint64_t times_visited;
+  uint64_t evals_to_first_find;
+} bk_minimum_family;
+
+typedef struct bk_collect_stats {
+  uint64_t total_starts;
+  uint64_t total_evals;
+  uint64_t batches;
+  int32_t saturated;
+  int32_t reserved;
+} bk_collect_stats;
+
+int bk_collect_minima(bk_ctx* ctx, int n, uint64_t seed, int64_t target_families, int64_t batch_size,
+                      int64_t max_starts, bk_minimum_family* out, int64_t capacity, int64_t* n_out,
+                      bk_collect_stats* stats);
+
 /* ---- Evolution (sampler.cuh:428-438, 451-457, 509-619, 149-195) ---- */
 
 typedef struct bk_evolve_params {
