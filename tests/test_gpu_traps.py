@@ -26,10 +26,10 @@ def test_device_descent_bit_exact(eng, n):
         fs, fe, ev = eng.steepest_descent(n, starts, budget)
         hs, he, hv = bk.steepest_descent(n, starts, budget)
         assert np.array_equal(fs, hs) and np.array_equal(fe, he) and np.array_equal(ev, hv)
-    if n <= 32:
-        for j in range(0, 777, 97):
-            r = O.steepest_descent(n, int(starts[j]), use_ref=True)
-            assert (int(fs[j]), int(fe[j]), int(ev[j])) == r[:3]
+        if n <= 32:
+            for j in range(0, 777, 97):
+                r = O.steepest_descent(n, int(starts[j]), max_evals=budget, use_ref=True)
+                assert (int(fs[j]), int(fe[j]), int(ev[j])) == r[:3]
 
 
 def _cpu_collect(n, seed, target, batch, max_starts):
