@@ -707,7 +707,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   BK_CUDA(c, cudaMemcpyAsync(base + o_slot, S.slot.data(), S.slot.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   if (!hab.empty())
     BK_CUDA(c, cudaMemcpyAsync(base + o_hab, hab.data(), hab.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
-  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R>), PersistSmem::kBytes));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R, true>), PersistSmem::kBytes));
   run->base = base;
   run->o_desc = o_desc;
   run->o_tasks = o_tasks;
@@ -755,7 +755,7 @@ int persist_launch(bk_ctx* c, PersistRun<R>& r, int k0, int n_steps, size_t n_fi
   if (P.n_steps == 0 && P.n_final == 0) return BK_OK;
   size_t ev = 0;
   BK_TRY(ev_begin(c, "persist", &ev));
-  persist_kernel<R><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
+  persist_kernel<R, true><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(
       reinterpret_cast<const InstDesc<R>*>(r.base + r.o_desc), P);
   BK_CUDA(c, cudaGetLastError());
   BK_TRY(ev_end(c, ev));
@@ -1112,7 +1112,7 @@ int evolve_batch_t(bk_ctx* c, const bk_batch_params* bp, const bk_batch_instance
     BK_CUDA(c, cudaMemcpyAsync(base + o_tab[kv.first], kv.second.data(), kv.second.size(), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_offs, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_idx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, st));
-  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R>), PersistSmem::kBytes));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R, false>), PersistSmem::kBytes));
 
   Program P{};
   P.tasks = reinterpret_cast<const unsigned long long*>(base + o_tasks);
@@ -1135,7 +1135,7 @@ int evolve_batch_t(bk_ctx* c, const bk_batch_params* bp, const bk_batch_instance
                                                                 reinterpret_cast<unsigned int*>(base + o_idx),
                                                                 c64 ? 1 : 0, n_inst);
     BK_CUDA(c, cudaGetLastError());
-    persist_kernel<R><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(dd, P);
+    persist_kernel<R, false><<<2 * c->num_sms, kPersistThreads, PersistSmem::kBytes, st>>>(dd, P);
     BK_CUDA(c, cudaGetLastError());
     return BK_OK;
   };

@@ -629,7 +629,10 @@ __device__ __forceinline__ bool dep_met(const unsigned int* ctr, uint32_t target
   return ctr == nullptr || seen >= target;
 }
 
-template <class R>
+// kCacheDesc: keep the running statevector's descriptor in shared memory (a
+// launch over one statevector); batched launches, whose consecutive tasks mostly
+// belong to different statevectors, read it from global memory instead.
+template <class R, bool kCacheDesc>
 __global__ void __launch_bounds__(kComputeThreads, 2)
     persist_kernel(const InstDesc<R>* __restrict__ insts, const Program P) {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -640,6 +643,9 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
   __shared__ uint32_t g_after;
   __shared__ int inflight;  // a tile load is issued and not yet consumed
   __shared__ int early;     // the current task's stage_free() issued the next load
+  __shared__ StageMeta after;  // the task after next, decoded while the current one computes
+  __shared__ __align__(16) InstDesc<R> sdesc;  // descriptor of the running task's statevector
+  __shared__ int sdesc_inst;
   unsigned char* stage = smem;
   unsigned char* phase_smem = smem + PersistSmem::kPhaseOff;
   double* red = reinterpret_cast<double*>(smem + PersistSmem::kRedOff);
@@ -652,6 +658,7 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
     mbar_init(fb, 1);
     fence_barrier_init();
     cur_phase_inst = -1;
+    sdesc_inst = -1;
     inflight = 0;
     const uint32_t g0 = atomicAdd(P.next, 1u);
     const uint32_t g1 = atomicAdd(P.next, 1u);
@@ -688,17 +695,35 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
     if (!mbar_wait_or_abort(fb, phase, P)) break;
     phase ^= 1u;
     if (tid == 0) inflight = 0;
-    const InstDesc<R>& D = insts[m.inst];
-    // stage free: issue the next task's load now if its dependency is met
+    if (kCacheDesc && m.inst != sdesc_inst) {
+      // the statevector changed: cache its descriptor in shared memory
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(insts + m.inst);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&sdesc);
+      for (int w = tid; w < (int)(sizeof(InstDesc<R>) / 4); w += kComputeThreads) dst[w] = src[w];
+      __syncthreads();
+      if (tid == 0) sdesc_inst = m.inst;
+    }
+    const InstDesc<R>& D = kCacheDesc ? sdesc : insts[m.inst];
+    // the counter this task completes, read now: the next task may replace the
+    // cached descriptor while warp 1 still signals this one
+    unsigned int* done_ctr = m.kind == TASK_A1 ? D.a1_done + (m.tile >> D.w2)
+                             : m.kind == TASK_S2 ? D.s2_done
+                             : m.kind == TASK_S3 ? D.s3_done
+                                                 : nullptr;
+    // stage free: issue the next task's load now if its dependency is met, and
+    // decode the task after next (its claim was issued at the top of the loop)
     auto stage_free = [&]() {
       if (tid == 0) {
         early = 0;
+        // a dependency not met at the top of the loop may be met by now
+        if (nxt.kind != TASK_END && nctr != nullptr && nseen < ntarget) nseen = ld_acquire(nctr);
         if (nxt.kind != TASK_END && dep_met<R>(nctr, ntarget, nseen)) {
           if (nctr) fence_proxy_async_global();
           issue_task_load(insts[nxt.inst], nxt, stage, fb);
           inflight = 1;
           early = 1;
         }
+        if (!decode_task<R>(P, g_after, after)) after.kind = TASK_END;
       }
     };
     if (m.kind == TASK_A1) {
@@ -727,16 +752,14 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
     if (tid == 0) {
       pending = (nxt.kind != TASK_END) && !early;
       cur = nxt;
-      if (!decode_task<R>(P, g_after, nxt)) nxt.kind = TASK_END;
+      nxt = after;
     }
     __syncthreads();  // publish cur
     if (tid == 32) {
       // completion of task m: the stores of every thread precede the barrier
       // above; this gpu-scope fence releases them together with the counter
       __threadfence();
-      if (m.kind == TASK_A1) atomicAdd(D.a1_done + (m.tile >> D.w2), 1u);
-      else if (m.kind == TASK_S2) atomicAdd(D.s2_done, 1u);
-      else if (m.kind == TASK_S3) atomicAdd(D.s3_done, 1u);
+      if (done_ctr) atomicAdd(done_ctr, 1u);
     }
     if (tid == 0 && pending) {
       const InstDesc<R>& D2 = insts[cur.inst];
