@@ -22,7 +22,6 @@
 
 #include "bk_adjoint.cuh"
 #include "bk_aux.cuh"
-#include "bk_cluster.cuh"
 #include "bk_engine.h"
 #include "bk_fused.cuh"
 #include "bk_persist.cuh"
@@ -782,68 +781,7 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
   const size_t o_desc = run.o_desc;
   InstDesc<R> D = run.D;
 
-  if (c->engine_mode == 2 && D.np == 27) {
-    // two passes per step on clusters of 8 CTAs (csrc/bk_cluster.cuh); pass H
-    // reads tiles of element bits [0, 3) u [15, 24), cluster = bits 3..14,
-    // rank = bits 24..26: its map replaces the S3 map slot
-    TmaDesc hm;
-    BK_TRY(build_amp_map(c, c->d_state, D.np, BK_C128, 3, 15, 9, &hm));
-    CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(const_cast<CUtensorMap*>(D.map_a1));
-    BK_CUDA(c, cudaMemcpyAsync(d_maps + 3, &hm.map, sizeof(CUtensorMap), cudaMemcpyHostToDevice, st));
-    InstDesc<R> DC = D;
-    DC.map_s2 = d_maps + 3;
-    DC.s2_mid_dim = hm.mid_dim;
-    DC.s2_hi_dim = hm.hi_dim;
-    DC.s2_mid_bits = (int)hm.mid_bits;
-    BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &DC, sizeof(DC), cudaMemcpyHostToDevice, st));
-    BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
-    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(cluster_pass_kernel<R>), PersistSmem::kBytes));
-    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_pass_kernel<R>), PersistSmem::kBytes));
-    const InstDesc<R>* dd = reinterpret_cast<const InstDesc<R>*>(base + o_desc);
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kClusterSize;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(n_a1);
-    cfg.blockDim = dim3(kComputeThreads);
-    cfg.dynamicSmemBytes = PersistSmem::kBytes;
-    cfg.stream = st;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int max_clusters = 0;
-    BK_CUDA(c, cudaOccupancyMaxActiveClusters(&max_clusters, cluster_pass_kernel<R>, &cfg));
-    if (max_clusters < 1) return fail(c, BK_ERR_UNSUPPORTED, "clusters of %d CTAs cannot be scheduled", kClusterSize);
-    using SampT = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
-    for (int k = 0; k <= p->n_steps; ++k) {
-      if (S.sample_pt[(size_t)k] >= 0)
-        BK_TRY(launch_sampling_t(c, reinterpret_cast<const SampT*>(c->d_state), n, S.sample_pt[(size_t)k], S.shots));
-      size_t ev = 0;
-      if (k == p->n_steps) {
-        if (S.slot[(size_t)k] >= 0) {
-          BK_TRY(ev_begin(c, "tile_m", &ev));
-          tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(dd, TASK_M, (uint32_t)k, err);
-          BK_CUDA(c, cudaGetLastError());
-          BK_TRY(ev_end(c, ev));
-        }
-        break;
-      }
-      BK_TRY(ev_begin(c, "cluster_l", &ev));
-      BK_CUDA(c, cudaLaunchKernelEx(&cfg, cluster_pass_kernel<R>, dd, 0, (uint32_t)k, err));
-      BK_TRY(ev_end(c, ev));
-      BK_TRY(ev_begin(c, "cluster_h", &ev));
-      BK_CUDA(c, cudaLaunchKernelEx(&cfg, cluster_pass_kernel<R>, dd, 1, (uint32_t)k, err));
-      BK_TRY(ev_end(c, ev));
-    }
-    int e = 0;
-    BK_CUDA(c, cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    BK_CUDA(c, cudaStreamSynchronize(st));
-    if (e != 0) return fail(c, BK_ERR_TIMEOUT, "cluster pass: a bounded device wait gave up (%d)", e);
-    return BK_OK;
-  }
-
-  if (c->engine_mode == 1 || c->engine_mode == 2) {
+  if (c->engine_mode == 1) {
     // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_pass_kernel<R>), PersistSmem::kBytes));
     using SampT = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
@@ -1942,7 +1880,7 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
   if (!c) return BK_ERR_INVALID;
   switch (option) {
     case BK_OPT_ENGINE_MODE:
-      if (value < 0 || value > 2) return fail(c, BK_ERR_INVALID, "engine mode %lld", (long long)value);
+      if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "engine mode %lld", (long long)value);
       c->engine_mode = (int)value;
       return BK_OK;
     case BK_OPT_SLAB_LAG:

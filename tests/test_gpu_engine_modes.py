@@ -71,22 +71,3 @@ def test_tuner_sweeps_and_caches(eng, tmp_path):
     assert eng.get_option("engine_mode") == e["best"]["engine_mode"]
     for k in tune.KNOBS:
         eng.set_option(k, {"engine_mode": 0, "slab_lag": 3, "split_w2": 0}[k])
-
-
-@pytest.mark.parametrize("n,precision,tol", [(28, bk.BK_C64, 1e-6), (27, bk.BK_C128, 1e-11)])
-def test_cluster_two_pass_mode(eng, n, precision, tol):
-    """Two passes per step on 8-CTA clusters (27 element bits) against the
-    three-pass per-pass schedule: the same rotations in another grouping, so
-    equal to rounding (complex64 1e-6, complex128 1e-11 over 20 steps)."""
-    bits, e0 = bk.select_trap(n, 42, 200, 0.01)
-    steps = 20
-    meas = list(range(0, steps + 1, 5))
-    out = []
-    for mode in (1, 2):
-        eng.set_option("engine_mode", mode)
-        out.append(eng.evolve(n, bits, 0.35, 0.02, steps, measure=meas, e0=e0, precision=precision))
-    eng.set_option("engine_mode", 0)
-    (p1, d1, n1), (p2, d2, n2) = out
-    assert np.max(np.abs(p1 - p2)) <= tol
-    assert np.max(np.abs(d1 - d2)) <= tol * n
-    assert np.max(np.abs(n2 - 1.0)) <= 100 * tol
