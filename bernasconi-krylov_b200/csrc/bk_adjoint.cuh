@@ -333,11 +333,11 @@ __device__ __forceinline__ void adj_issue(const AdjDesc<R>& D, int kind, uint32_
 // last_pass: the step's last pass also reduces the step's per-tile sums.
 template <class R>
 __global__ void __launch_bounds__(kComputeThreads, 1)
-    adj_pass_kernel(const AdjDesc<R>* __restrict__ dd, int kind, uint32_t j, int phase_on, int last_pass, int* err) {
+    adj_pass_kernel(const __grid_constant__ AdjDesc<R> D, int kind, uint32_t j, int phase_on, int last_pass,
+                    int* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t full_bar;
   __shared__ int is_last;
-  const AdjDesc<R>& D = *dd;
   unsigned char* stage = smem;
   unsigned char* phase_smem = smem + AdjSmem::kPhaseOff;
   double* red = reinterpret_cast<double*>(smem + AdjSmem::kRedOff);
@@ -350,14 +350,15 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
   const int mb = kind == TASK_S2 ? D.s2_mid_bits : D.s3_mid_bits;
   // qubits rotated by the earlier passes of the step (complex64: + amplitude bit 0)
   const int m0 = (sizeof(R) == 4 ? 1 : 0) + kElemBits + (kind == TASK_S3 ? D.w2 : 0);
+  uint32_t tile = blockIdx.x;
+  // the first tile's loads go out before the phase tables are staged
   if (tid == 0) {
     mbar_init(fb, 1);
     fence_barrier_init();
+    if (tile < ntiles) adj_issue(D, kind, tile, stage, fb);
   }
   if (kind == TASK_A1 && phase_on) PhaseV<R>::stage(D.phase, phase_smem, tid, kComputeThreads);
   __syncthreads();
-  uint32_t tile = blockIdx.x;
-  if (tid == 0 && tile < ntiles) adj_issue(D, kind, tile, stage, fb);
   uint32_t parity = 0;
   for (; tile < ntiles; tile += gridDim.x) {
     const bool ok = mbar_wait_bounded(fb, parity, err);

@@ -795,23 +795,23 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
       if (k == p->n_steps) {
         if (S.slot[(size_t)k] >= 0) {
           BK_TRY(ev_begin(c, "tile_m", &ev));
-          tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(dd, TASK_M, (uint32_t)k, err);
+          tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_M, (uint32_t)k, err);
           BK_CUDA(c, cudaGetLastError());
           BK_TRY(ev_end(c, ev));
         }
         break;
       }
       BK_TRY(ev_begin(c, "tile_a1", &ev));
-      tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(dd, TASK_A1, (uint32_t)k, err);
+      tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_A1, (uint32_t)k, err);
       BK_CUDA(c, cudaGetLastError());
       BK_TRY(ev_end(c, ev));
       BK_TRY(ev_begin(c, "tile_s2", &ev));
-      tile_pass_kernel<R><<<n_s2, kComputeThreads, PersistSmem::kBytes, st>>>(dd, TASK_S2, (uint32_t)k, err);
+      tile_pass_kernel<R><<<n_s2, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_S2, (uint32_t)k, err);
       BK_CUDA(c, cudaGetLastError());
       BK_TRY(ev_end(c, ev));
       if (n_s3 > 0) {
         BK_TRY(ev_begin(c, "tile_s3", &ev));
-        tile_pass_kernel<R><<<n_s3, kComputeThreads, PersistSmem::kBytes, st>>>(dd, TASK_S3, (uint32_t)k, err);
+        tile_pass_kernel<R><<<n_s3, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_S3, (uint32_t)k, err);
         BK_CUDA(c, cudaGetLastError());
         BK_TRY(ev_end(c, ev));
       }
@@ -1469,7 +1469,6 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   const uint32_t n_a1 = FD.n_a1, n_s2 = FD.n_s2, n_s3 = FD.n_s3;
   Bump b;
   const size_t o_maps = b.take(7 * sizeof(CUtensorMap));
-  const size_t o_desc = b.take(sizeof(AdjDesc<R>));
   const size_t o_tan = b.take((size_t)T * sizeof(R));
   const size_t o_sc = b.take((size_t)T * sizeof(R));
   const size_t o_lg = b.take((size_t)T * sizeof(double));
@@ -1528,13 +1527,11 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   A.n_s2 = n_s2;
   A.n_s3 = n_s3;
   BK_CUDA(c, cudaMemcpyAsync(d_maps, maps, sizeof(maps), cudaMemcpyHostToDevice, st));
-  BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &A, sizeof(A), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_tan, t_rev.data(), (size_t)T * sizeof(R), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_sc, sc_rev.data(), (size_t)T * sizeof(R), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_lg, lg_rev.data(), (size_t)T * sizeof(double), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemsetAsync(base + o_ctr, 0, 64, st));
   BK_TRY(allow_smem(c, reinterpret_cast<const void*>(adj_pass_kernel<R>), AdjSmem::kBytes));
-  const AdjDesc<R>* dd = reinterpret_cast<const AdjDesc<R>*>(base + o_desc);
   const int ns = c->num_sms;
   const unsigned g1 = std::min<unsigned>(n_a1, (unsigned)ns), g2 = std::min<unsigned>(n_s2, (unsigned)ns),
                  g3 = std::min<unsigned>(std::max<unsigned>(n_s3, 1u), (unsigned)ns);
@@ -1551,16 +1548,16 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   for (int j = 0; j < T; ++j) {
     size_t e = 0;
     BK_TRY(ev_begin(c, "adj_a1", &e));
-    adj_pass_kernel<R><<<g1, kComputeThreads, AdjSmem::kBytes, st>>>(dd, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0, err);
+    adj_pass_kernel<R><<<g1, kComputeThreads, AdjSmem::kBytes, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0, err);
     BK_CUDA(c, cudaGetLastError());
     BK_TRY(ev_end(c, e));
     BK_TRY(ev_begin(c, "adj_s2", &e));
-    adj_pass_kernel<R><<<g2, kComputeThreads, AdjSmem::kBytes, st>>>(dd, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1, err);
+    adj_pass_kernel<R><<<g2, kComputeThreads, AdjSmem::kBytes, st>>>(A, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1, err);
     BK_CUDA(c, cudaGetLastError());
     BK_TRY(ev_end(c, e));
     if (w3 > 0) {
       BK_TRY(ev_begin(c, "adj_s3", &e));
-      adj_pass_kernel<R><<<g3, kComputeThreads, AdjSmem::kBytes, st>>>(dd, TASK_S3, (uint32_t)j, 0, 1, err);
+      adj_pass_kernel<R><<<g3, kComputeThreads, AdjSmem::kBytes, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
       BK_CUDA(c, cudaGetLastError());
       BK_TRY(ev_end(c, e));
     }

@@ -780,11 +780,13 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
 // ---------------------------------------------------------------------------
 // Grid variant: one CTA per tile of one pass (kind = TASK_A1 / TASK_S2 /
 // TASK_S3 / TASK_M), no dependencies (the kernel boundary orders the passes).
-// Same tile arithmetic as the persistent engine; blockIdx.x is the tile.
+// Same tile arithmetic as the persistent engine; blockIdx.x is the tile. The
+// descriptor is a kernel parameter (constant bank), so the TMA coordinates need
+// no dependent global loads.
 // ---------------------------------------------------------------------------
 template <class R>
 __global__ void __launch_bounds__(kComputeThreads, 2)
-    tile_pass_kernel(const InstDesc<R>* __restrict__ insts, int kind, uint32_t step, int* err) {
+    tile_pass_kernel(const __grid_constant__ InstDesc<R> D, int kind, uint32_t step, int* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t full_bar;
   __shared__ int last_flag;
@@ -793,19 +795,19 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
   double* red = reinterpret_cast<double*>(smem + PersistSmem::kRedOff);
   const int tid = threadIdx.x;
   const uint32_t fb = smem_addr(&full_bar);
-  const InstDesc<R>& D = insts[0];
   StageMeta m;
   m.kind = kind;
   m.inst = 0;
   m.tile = blockIdx.x;
   m.step = step;
+  // the tile load goes out first; the phase tables are staged while it is in flight
   if (tid == 0) {
     mbar_init(fb, 1);
     fence_barrier_init();
+    issue_task_load(D, m, stage, fb);
   }
   if (kind == TASK_A1) PhaseV<R>::stage(D.phase, phase_smem, tid, kComputeThreads);
   __syncthreads();
-  if (tid == 0) issue_task_load(D, m, stage, fb);
   const bool ok = mbar_wait_bounded(fb, 0, err);
   if (__syncthreads_or(!ok)) return;
   auto none = []() {};
