@@ -166,9 +166,11 @@ __device__ __forceinline__ double adj_a1(unsigned char* sp, unsigned char* sl, c
 #pragma unroll
   for (int q = 0; q < 16; ++q) {
     if (phase_on) {
+      // one set of rotation coefficients for both statevectors
       const uint32_t e = load_e<R>(etile, b1 | pdep((uint32_t)q, PL::A1_R1_REG));
-      PhaseV<R>::apply(v[q], e, D.phase, phase_smem, true);
-      PhaseV<R>::apply(u[q], e, D.phase, phase_smem, true);
+      const typename PhaseV<R>::Coef cf = PhaseV<R>::coef(e, D.phase, phase_smem, true);
+      PhaseV<R>::rotate(v[q], cf, true);
+      PhaseV<R>::rotate(u[q], cf, true);
     }
     if (sc != (R)1) {
       E::scale(v[q], sc);

@@ -734,7 +734,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
 // measurement-only tasks (0 or all of them) for step k0 + n_steps; waits for the
 // launch and reports a bounded device wait that gave up.
 template <class R>
-int persist_launch(bk_ctx* c, PersistRun<R>& r, int k0, int n_steps, size_t n_final) {
+int persist_launch(bk_ctx* c, PersistRun<R>& r, int k0, int n_steps, size_t n_final, bool wait = true) {
   cudaStream_t st = c->stream;
   InstDesc<R> D = r.D;
   D.tan = reinterpret_cast<const R*>(r.base + r.o_tan) + k0;
@@ -759,6 +759,7 @@ int persist_launch(bk_ctx* c, PersistRun<R>& r, int k0, int n_steps, size_t n_fi
       reinterpret_cast<const InstDesc<R>*>(r.base + r.o_desc), P);
   BK_CUDA(c, cudaGetLastError());
   BK_TRY(ev_end(c, ev));
+  if (!wait) return BK_OK;  // the caller reads r.err after its own synchronisation
   int e = 0;
   BK_CUDA(c, cudaMemcpyAsync(&e, r.err, sizeof(int), cudaMemcpyDeviceToHost, st));
   BK_CUDA(c, cudaStreamSynchronize(st));
@@ -1401,33 +1402,47 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   PersistRun<R> run;
   BK_TRY(persist_prepare<R>(c, &q, S, angle_unit, tans, scales, &run));
   unsigned char* ckpt = static_cast<unsigned char*>(c->d_ckpt);
-  BK_CUDA(c, cudaEventRecord(ev[0], st));
-  for (int w = 0; w <= n_ckpt; ++w) {
-    const int k0 = w * K, k1 = (w == n_ckpt) ? T : (w + 1) * K;
-    if (w > 0)
-      BK_CUDA(c, cudaMemcpyAsync(ckpt + (size_t)(w - 1) * sbytes, c->d_state, sbytes, cudaMemcpyDeviceToDevice, st));
-    BK_TRY(persist_launch<R>(c, run, k0, k1 - k0, (w == n_ckpt) ? run.n_final : 0));
-  }
-  BK_CUDA(c, cudaEventRecord(ev[1], st));
-  double row[4] = {0, 0, 0, 0};
-  BK_CUDA(c, cudaMemcpyAsync(row, c->d_results, sizeof(row), cudaMemcpyDeviceToHost, st));
-  BK_CUDA(c, cudaStreamSynchronize(st));
-  const long double f = std::exp2(-2.0L * lgf[(size_t)T]);
-  const double value = (double)((long double)row[p->objective == BK_OBJ_P_LESS ? 0 : 1] * f);
-  if (value_out) *value_out = value;
   grad_step->assign((size_t)T, 0.0);
-  float fw_ms = 0.f;
-  BK_CUDA(c, cudaEventElapsedTime(&fw_ms, ev[0], ev[1]));
-  if (stats) {
-    stats->value = value;
-    stats->norm = (double)((long double)row[2] * f);
-    stats->checkpoint_every = K;
-    stats->n_checkpoints = n_ckpt;
-    stats->max_drift = 0.0;
-    stats->forward_ms = fw_ms;
-    stats->reverse_ms = 0.0;
+  // forward: one persistent launch per window of K steps, psi copied to a
+  // checkpoint between windows; enqueued without host synchronisation
+  auto enqueue_forward = [&]() -> int {
+    BK_CUDA(c, cudaEventRecord(ev[0], st));
+    for (int w = 0; w <= n_ckpt; ++w) {
+      const int k0 = w * K, k1 = (w == n_ckpt) ? T : (w + 1) * K;
+      if (w > 0)
+        BK_CUDA(c, cudaMemcpyAsync(ckpt + (size_t)(w - 1) * sbytes, c->d_state, sbytes, cudaMemcpyDeviceToDevice, st));
+      BK_TRY(persist_launch<R>(c, run, k0, k1 - k0, (w == n_ckpt) ? run.n_final : 0, false));
+    }
+    BK_CUDA(c, cudaEventRecord(ev[1], st));
+    return BK_OK;
+  };
+  double row[4] = {0, 0, 0, 0};
+  int e_fwd = 0;
+  auto finish_forward = [&]() -> int {
+    if (e_fwd != 0) return fail(c, BK_ERR_TIMEOUT, "persistent engine: a bounded device wait gave up (%d)", e_fwd);
+    const long double f = std::exp2(-2.0L * lgf[(size_t)T]);
+    const double value = (double)((long double)row[p->objective == BK_OBJ_P_LESS ? 0 : 1] * f);
+    if (value_out) *value_out = value;
+    float fw_ms = 0.f;
+    BK_CUDA(c, cudaEventElapsedTime(&fw_ms, ev[0], ev[1]));
+    if (stats) {
+      stats->value = value;
+      stats->norm = (double)((long double)row[2] * f);
+      stats->checkpoint_every = K;
+      stats->n_checkpoints = n_ckpt;
+      stats->max_drift = 0.0;
+      stats->forward_ms = fw_ms;
+      stats->reverse_ms = 0.0;
+    }
+    return BK_OK;
+  };
+  if (T == 0) {
+    BK_TRY(enqueue_forward());
+    BK_CUDA(c, cudaMemcpyAsync(row, c->d_results, sizeof(row), cudaMemcpyDeviceToHost, st));
+    BK_CUDA(c, cudaMemcpyAsync(&e_fwd, run.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BK_CUDA(c, cudaStreamSynchronize(st));
+    return finish_forward();
   }
-  if (T == 0) return BK_OK;
 
   // reverse-sweep bookkeeping on the host: tangents, rescales, round-weight
   // logs, the log2 scale of both vectors at each step's cross terms, resets
@@ -1536,6 +1551,8 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   const unsigned g1 = std::min<unsigned>(n_a1, (unsigned)ns), g2 = std::min<unsigned>(n_s2, (unsigned)ns),
                  g3 = std::min<unsigned>(std::max<unsigned>(n_s3, 1u), (unsigned)ns);
 
+  // the whole gradient goes to the device back to back: forward, then the sweep
+  BK_TRY(enqueue_forward());
   BK_CUDA(c, cudaEventRecord(ev[2], st));
   {
     const unsigned grid = (unsigned)std::min<size_t>((n_el + 255) / 256, (size_t)kResetGrid);
@@ -1580,7 +1597,11 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
     BK_CUDA(c, cudaMemcpyAsync(dev.data(), d_dev, resets.size() * kResetGrid * sizeof(double),
                                cudaMemcpyDeviceToHost, st));
   BK_CUDA(c, cudaMemcpyAsync(&e_dev, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  // the forward's result row is untouched by the sweep: read it with the rest
+  BK_CUDA(c, cudaMemcpyAsync(row, c->d_results, sizeof(row), cudaMemcpyDeviceToHost, st));
+  BK_CUDA(c, cudaMemcpyAsync(&e_fwd, run.err, sizeof(int), cudaMemcpyDeviceToHost, st));
   BK_CUDA(c, cudaStreamSynchronize(st));
+  BK_TRY(finish_forward());
   if (e_dev != 0) return fail(c, BK_ERR_TIMEOUT, "adjoint sweep: a bounded device wait gave up (%d)", e_dev);
   BK_TRY(collect_timing(c));
   for (int j = 0; j < T; ++j) {

@@ -160,8 +160,11 @@ struct PhaseV<float> {
     y = __ffma2_rn(b, x, y);
     x = __ffma2_rn(a, y, x);
   }
-  __device__ static void apply(El<float>::T& v, uint32_t e2, const PhaseV32& P, const unsigned char* s,
-                               bool inverse) {
+  // the rotation coefficients of an element (two amplitudes); inverse: negated
+  struct Coef {
+    float2 a, b, A, B;
+  };
+  __device__ static Coef coef(uint32_t e2, const PhaseV32& P, const unsigned char* s, bool inverse) {
     const float2* hab = reinterpret_cast<const float2*>(s);
     const uint32_t e0 = e2 & 0xFFFFu, e1 = e2 >> 16;
     const uint32_t h0 = __umulhi(e0, P.M), h1 = __umulhi(e1, P.M);
@@ -176,29 +179,41 @@ struct PhaseV<float> {
     tt = __ffma2_rn(x2, tt, make_float2(2.0f / 15.0f, 2.0f / 15.0f));
     tt = __ffma2_rn(x2, tt, make_float2(1.0f / 3.0f, 1.0f / 3.0f));
     tt = __ffma2_rn(x2, tt, make_float2(1.0f, 1.0f));
-    float2 a = __fmul2_rn(make_float2(-x.x, -x.y), tt);
+    Coef c;
+    c.a = __fmul2_rn(make_float2(-x.x, -x.y), tt);
     const float2 r2 = __fmul2_rn(r, r);
     float2 u = __ffma2_rn(r2, make_float2(1.0f / 362880.0f, 1.0f / 362880.0f), make_float2(-1.0f / 5040.0f, -1.0f / 5040.0f));
     u = __ffma2_rn(r2, u, make_float2(1.0f / 120.0f, 1.0f / 120.0f));
     u = __ffma2_rn(r2, u, make_float2(-1.0f / 6.0f, -1.0f / 6.0f));
     u = __ffma2_rn(r2, u, make_float2(1.0f, 1.0f));
-    float2 b = __fmul2_rn(r, u);
+    c.b = __fmul2_rn(r, u);
     const float2 H0 = hab[h0], H1 = hab[h1];
-    float2 A = make_float2(H0.x, H1.x), B = make_float2(H0.y, H1.y);
-    if (!inverse) {
-      shear2(v.re, v.im, a, b);
-      shear2(v.re, v.im, A, B);
-      shear2(v.re, v.im, A, B);
-    } else {
-      // inverse: the same shears with negated coefficients in reverse order
-      A = make_float2(-A.x, -A.y);
-      B = make_float2(-B.x, -B.y);
-      a = make_float2(-a.x, -a.y);
-      b = make_float2(-b.x, -b.y);
-      shear2(v.re, v.im, A, B);
-      shear2(v.re, v.im, A, B);
-      shear2(v.re, v.im, a, b);
+    c.A = make_float2(H0.x, H1.x);
+    c.B = make_float2(H0.y, H1.y);
+    if (inverse) {
+      c.A = make_float2(-c.A.x, -c.A.y);
+      c.B = make_float2(-c.B.x, -c.B.y);
+      c.a = make_float2(-c.a.x, -c.a.y);
+      c.b = make_float2(-c.b.x, -c.b.y);
     }
+    return c;
+  }
+  // forward: residual shear then the level shear twice; inverse: the negated
+  // shears in reverse order
+  __device__ static void rotate(El<float>::T& v, const Coef& c, bool inverse) {
+    if (!inverse) {
+      shear2(v.re, v.im, c.a, c.b);
+      shear2(v.re, v.im, c.A, c.B);
+      shear2(v.re, v.im, c.A, c.B);
+    } else {
+      shear2(v.re, v.im, c.A, c.B);
+      shear2(v.re, v.im, c.A, c.B);
+      shear2(v.re, v.im, c.a, c.b);
+    }
+  }
+  __device__ static void apply(El<float>::T& v, uint32_t e2, const PhaseV32& P, const unsigned char* s,
+                               bool inverse) {
+    rotate(v, coef(e2, P, s, inverse), inverse);
   }
 };
 template <>
@@ -211,14 +226,21 @@ struct PhaseV<double> {
     for (int i = tid; i < P.n_hi; i += nthr) hi[i] = P.hi[i];
     for (int i = tid; i < kPhaseLo; i += nthr) lo[i] = P.lo[i];
   }
-  __device__ static void apply(El<double>::T& v, uint32_t e, const PhaseV64&, const unsigned char* s,
-                               bool inverse) {
+  using Coef = double2;  // (cos, sin) of the rotation
+  __device__ static Coef coef(uint32_t e, const PhaseV64&, const unsigned char* s, bool inverse) {
     const double2* hi = reinterpret_cast<const double2*>(s);
     const double2* lo = hi + kPhaseHi64;
     const double2 h = hi[e >> kPhaseLoBits], l = lo[e & (kPhaseLo - 1)];
     const double c = fma(h.x, l.x, -h.y * l.y);
     const double sn = inverse ? -fma(h.x, l.y, h.y * l.x) : fma(h.x, l.y, h.y * l.x);
-    v.v = make_double2(fma(v.v.x, c, -v.v.y * sn), fma(v.v.x, sn, v.v.y * c));
+    return make_double2(c, sn);
+  }
+  __device__ static void rotate(El<double>::T& v, const Coef& cs, bool) {
+    v.v = make_double2(fma(v.v.x, cs.x, -v.v.y * cs.y), fma(v.v.x, cs.y, v.v.y * cs.x));
+  }
+  __device__ static void apply(El<double>::T& v, uint32_t e, const PhaseV64& P, const unsigned char* s,
+                               bool inverse) {
+    rotate(v, coef(e, P, s, inverse), inverse);
   }
 };
 
