@@ -177,6 +177,28 @@ def run_reference(a):
     print(json.dumps(line))
 
 
+def replica_trap(n, rank, n_descents=4000, quantile=0.01):
+    """Trap of one replica: the lowest `quantile` of `n_descents` seeded descents, seed 42 + rank."""
+    import bk_b200 as bk
+    return bk.select_trap(n, 42 + rank, n_descents, quantile)
+
+
+def max_over_ranks(x, world, device):
+    """Largest value over all ranks (the job's time is its slowest rank's)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(units_per_rank, world, seconds_max):
+    """Weak scaling: every rank processes units_per_rank; the job ends with its slowest rank."""
+    return units_per_rank * world / seconds_max
+
+
 def tuned_knobs(eng, a, n, prec, trap):
     """Engine knobs for this run: explicit flags, else the autotuner's cached choice
     for this device and size, else a tuning sweep now (not timed, not cached)."""
@@ -357,17 +379,11 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     n, T = a.n, a.trotter
     prec = bk.BK_C64 if a.precision == "c64" else bk.BK_C128
     eng = bk.Engine(local)
-    bits, e0 = bk.select_trap(n, 42 + rank, 4000, 0.01)
+    bits, e0 = replica_trap(n, rank)
     tuning = tuned_knobs(eng, a, n, prec, (bits, e0))
     meas = list(range(0, T + 1, a.measure_every))
     dev = torch.device("cuda", local)
@@ -395,7 +411,7 @@ def main():
     dev_s = ev0.elapsed_time(ev1) / 1e3
     timing = eng.kernel_timing()
     eng.set_kernel_timing(False)
-    dev_s_max = max_over_ranks(dev_s)
+    dev_s_max = max_over_ranks(dev_s, world, f"cuda:{local}")
 
     # ---- end-to-end region: the C-ABI call with host buffers, wall clock ----
     barrier()
@@ -405,11 +421,11 @@ def main():
         bench_step()
     torch.cuda.synchronize(dev)
     barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, f"cuda:{local}")
 
     amp_steps = float(1 << n) * T * a.steps * world
-    value = amp_steps / dev_s_max
-    e2e = amp_steps / e2e_s
+    value = whole_job_value(float(1 << n) * T * a.steps, world, dev_s_max)
+    e2e = whole_job_value(float(1 << n) * T * a.steps, world, e2e_s)
 
     # ---- roofline of the dominant kernel ----
     S = 8 if prec == bk.BK_C64 else 16

@@ -124,3 +124,16 @@ def test_adjoint_rejects_bad_input(eng):
     with pytest.raises(bk.BkError) as e:
         eng.adjoint(16, 5, [0.3, 0.4], 0.05, 4, segment_of_step=[0, 1, 2, 0], precision=bk.BK_C64)
     assert e.value.status == bk._lib.BK_ERR_INVALID
+
+
+def test_adjoint_n28_complex64_against_complex128(eng):
+    """The large configuration's adjoint: N = 28 (three-pass dual sweep, S2 + S3),
+    checkpoints every 16 steps; complex64 gradients within 1e-3 of complex128."""
+    n, T, nseg = 28, 64, 4
+    bits, e0 = bk.select_trap(n, 42, 200, 0.01)
+    gs = np.random.default_rng(28).uniform(0.25, 0.45, nseg)
+    v64, g64, st64 = eng.adjoint(n, bits, gs, 0.02, T, e0=e0, precision=bk.BK_C64, checkpoint_every=16)
+    v128, g128, st128 = eng.adjoint(n, bits, gs, 0.02, T, e0=e0, precision=bk.BK_C128, checkpoint_every=16)
+    assert st64["n_checkpoints"] == 3 and st128["max_drift"] <= 1e-11 and st64["max_drift"] <= 1e-4
+    assert abs(v64 - v128) <= 1e-6
+    assert np.max(np.abs(g64 - g128)) <= 1e-3 * np.max(np.abs(g128))
