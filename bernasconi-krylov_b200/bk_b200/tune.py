@@ -5,7 +5,9 @@ Knobs (engine options, include/bk_engine.h):
   engine_mode  0 = persistent dataflow kernel (every step in one launch, A1 tiles
                handed to S2 through L2), 1 = one grid launch per pass;
   slab_lag     persistent engine: slabs between a slab's A1 and S2 tasks;
-  split_w2     qubits of the S2 pass (the rest go to S3), 0 = engine default.
+  split_w2     qubits of the S2 pass (the rest go to S3), 0 = engine default;
+  e_source     E(s) for the diagonal phase: 0 = uint16 table, 1 = recomputed
+               from popcounts in the pass (no E traffic, more arithmetic).
 For the batched engine the knob is the task-block lag between a statevector
 slab's A1 and S2 tasks.
 
@@ -24,7 +26,8 @@ import os
 from ._lib import BK_C64, BK_C128
 
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.json")
-KNOBS = ("engine_mode", "slab_lag", "split_w2")
+KNOBS = ("engine_mode", "slab_lag", "split_w2", "e_source")
+DEFAULTS = {"engine_mode": 0, "slab_lag": 3, "split_w2": 0, "e_source": 0}
 ELEM_BITS = 12  # element bits of one 64 KB tile
 
 
@@ -47,14 +50,17 @@ def candidates(n, precision):
     np_ = n - 1 if precision == BK_C64 else n
     rest = np_ - ELEM_BITS
     if rest < 1:
-        return [dict(engine_mode=0, slab_lag=3, split_w2=0)]
+        return [dict(DEFAULTS)]
     d = default_w2(rest)
     widths = [0] + [w for w in (d - 1, d + 1) if 1 <= w <= 9 and w <= rest and rest - w <= 9]
     out = []
     for w in widths:
-        out.append(dict(engine_mode=1, slab_lag=3, split_w2=w))
+        out.append(dict(engine_mode=1, slab_lag=3, split_w2=w, e_source=0))
         for lag in (1, 2, 3, 4, 6):
-            out.append(dict(engine_mode=0, slab_lag=lag, split_w2=w))
+            out.append(dict(engine_mode=0, slab_lag=lag, split_w2=w, e_source=0))
+    # E recomputed in the pass, on the default split of both schedules
+    out.append(dict(engine_mode=1, slab_lag=3, split_w2=0, e_source=1))
+    out.append(dict(engine_mode=0, slab_lag=3, split_w2=0, e_source=1))
     return out
 
 
@@ -74,7 +80,7 @@ def _timer(eng):
 
 def apply_config(eng, cfg):
     for k in KNOBS:
-        eng.set_option(k, int(cfg[k]))
+        eng.set_option(k, int(cfg.get(k, DEFAULTS[k])))
 
 
 def measure(eng, n, precision, cfg, bits, e0, steps=20, warmup=4, g=0.35, dt=0.02):

@@ -91,6 +91,7 @@ struct bk_ctx {
   int slab_lag = 3;           // persistent engine: S2 queue lag behind A1, in slabs
   int engine_mode = 0;        // 0 persistent dataflow, 1 one launch per pass (tile grid)
   int force_w2 = 0;           // S2 width when > 0 and valid for the size (else the default split)
+  int e_recompute = 0;        // tile engine: 1 = E(s) recomputed from popcounts in A1, 0 = uint16 table
   std::map<int, uint16_t*> batch_E;  // E tables of batched runs, per n
   void* d_batch_state = nullptr;
   size_t batch_state_cap = 0;
@@ -693,7 +694,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   D.n_a1 = n_a1;
   D.n_s2 = n_s2;
   D.n_s3 = n_s3;
-  D.inverse = 0;
+  D.e_recompute = c->e_recompute;
 
   cudaStream_t st = c->stream;
   BK_CUDA(c, cudaMemcpyAsync(d_maps, maps, sizeof(maps), cudaMemcpyHostToDevice, st));
@@ -1093,7 +1094,7 @@ int evolve_batch_t(bk_ctx* c, const bk_batch_params* bp, const bk_batch_instance
     D.n_a1 = g.n_a1;
     D.n_s2 = g.n_a1;
     D.n_s3 = g.w3 > 0 ? g.n_a1 : 0u;
-    D.inverse = 0;
+    D.e_recompute = c->e_recompute;
     descs[(size_t)i] = D;
     offs[(size_t)i] = g.state_off;
     idx[(size_t)i] = g.s0;
@@ -1909,6 +1910,10 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
       if (value < 0 || value > 9) return fail(c, BK_ERR_INVALID, "S2 width %lld", (long long)value);
       c->force_w2 = (int)value;
       return BK_OK;
+    case BK_OPT_E_SOURCE:
+      if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "E source %lld", (long long)value);
+      c->e_recompute = (int)value;
+      return BK_OK;
     default:
       return fail(c, BK_ERR_INVALID, "unknown option %d", option);
   }
@@ -1920,6 +1925,7 @@ int bk_get_option(const bk_ctx* c, int option, int64_t* value) {
     case BK_OPT_ENGINE_MODE: *value = c->engine_mode; return BK_OK;
     case BK_OPT_SLAB_LAG: *value = c->slab_lag; return BK_OK;
     case BK_OPT_SPLIT_W2: *value = c->force_w2; return BK_OK;
+    case BK_OPT_E_SOURCE: *value = c->e_recompute; return BK_OK;
     default: return BK_ERR_INVALID;
   }
 }

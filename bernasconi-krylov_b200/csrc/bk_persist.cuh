@@ -273,7 +273,7 @@ struct InstDesc {
   double* partials;              // [A1 tiles][3]
   double* results;               // [rows][4]
   uint32_t n_a1, n_s2, n_s3;     // tiles per step
-  int inverse;                   // reserved
+  int e_recompute;               // 1: A1 / M recompute E(s) from popcounts instead of reading the E tile
 };
 
 struct Program {
@@ -371,6 +371,17 @@ __device__ __forceinline__ void measure_el(MeasureAcc& acc, const El<double>::T&
                                            int e0, uint32_t s0) {
   acc.add(fma(v.v.x, v.v.x, v.v.y * v.v.y), (int)e < e0, __popc(elem_g ^ s0));
 }
+// E of a 16-byte element recomputed in integers (complex64: both amplitudes
+// packed like the table's uint32 pair)
+template <class R>
+__device__ __forceinline__ uint32_t recompute_e(uint32_t elem_g, int n) {
+  if constexpr (sizeof(R) == 4) {
+    const uint32_t a0 = elem_g << 1;
+    return (uint32_t)labs_energy(a0, n) | ((uint32_t)labs_energy(a0 | 1u, n) << 16);
+  } else {
+    return (uint32_t)labs_energy(elem_g, n);
+  }
+}
 template <class R>
 __device__ __forceinline__ uint32_t load_e(const unsigned char* etile, uint32_t elem) {
   if constexpr (sizeof(R) == 4)
@@ -460,7 +471,10 @@ __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned c
     // measurement only: read the E values first, then release the stage
     uint32_t ev[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) ev[j] = load_e<R>(etile, b1 | pdep((uint32_t)j, PL::A1_R1_REG));
+    for (int j = 0; j < 16; ++j) {
+      const uint32_t i = b1 | pdep((uint32_t)j, PL::A1_R1_REG);
+      ev[j] = D.e_recompute ? recompute_e<R>(tile_base | i, D.n) : load_e<R>(etile, i);
+    }
     __syncthreads();
     stage_free();
 #pragma unroll
@@ -469,7 +483,7 @@ __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned c
 #pragma unroll
   for (int j = 0; j < 16 && !MEASURE_ONLY; ++j) {
     const uint32_t i = b1 | pdep((uint32_t)j, PL::A1_R1_REG);
-    const uint32_t e = load_e<R>(etile, i);
+    const uint32_t e = D.e_recompute ? recompute_e<R>(tile_base | i, D.n) : load_e<R>(etile, i);
     if (slot >= 0) measure_el(acc, v[j], e, tile_base | i, D.e0, D.s0);
     if (!MEASURE_ONLY) {
       PhaseV<R>::apply(v[j], e, D.phase, phase_smem, false);
@@ -612,12 +626,13 @@ template <class R>
 __device__ __forceinline__ void issue_task_load(const InstDesc<R>& D, const StageMeta& m, unsigned char* stage,
                                                 uint32_t fb) {
   if (m.kind == TASK_A1 || m.kind == TASK_M) {
-    mbar_arrive_expect_tx(fb, (uint32_t)(kStageTileBytes + 4096 * 2 * El<R>::kAmps));
+    const bool e_tile = !D.e_recompute;
+    mbar_arrive_expect_tx(fb, (uint32_t)kStageTileBytes + (e_tile ? 4096u * 2u * (uint32_t)El<R>::kAmps : 0u));
     const int hd = D.a1_hi_dim;
     const uint64_t pol = policy_evict_first();
     tma_load_5d_hint(smem_addr(stage), D.map_a1, 0, 0, hd == 2 ? (int)m.tile : 0, hd == 3 ? (int)m.tile : 0, 0, fb,
                      pol);
-    tma_load_5d_hint(smem_addr(stage + kStageTileBytes), D.map_e, 0, 0, (int)m.tile, 0, 0, fb, pol);
+    if (e_tile) tma_load_5d_hint(smem_addr(stage + kStageTileBytes), D.map_e, 0, 0, (int)m.tile, 0, 0, fb, pol);
   } else {
     const bool s2 = (m.kind == TASK_S2);
     const int mb = s2 ? D.s2_mid_bits : D.s3_mid_bits;

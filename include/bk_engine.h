@@ -269,8 +269,11 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       L2 hand-off between the A1 and S2 tasks), 1 = one grid launch per pass;
  *   BK_OPT_SLAB_LAG: persistent engine, slabs between A1 and S2 of a slab (>= 1);
  *   BK_OPT_SPLIT_W2: qubits of the S2 pass (1..9; the rest go to S3, at most 9),
- *       0 = the engine's default split; a width that does not fit a size is ignored. */
-enum { BK_OPT_ENGINE_MODE = 0, BK_OPT_SLAB_LAG = 1, BK_OPT_SPLIT_W2 = 2 };
+ *       0 = the engine's default split; a width that does not fit a size is ignored;
+ *   BK_OPT_E_SOURCE: where the diagonal phase and P_< get E(s): 0 = the cached
+ *       uint16 table (read with the A1 tile), 1 = recomputed in the pass from the
+ *       popcount form C_k = (n-k) - 2 popcount((x ^ (x >> k)) & (2^(n-k) - 1)). */
+enum { BK_OPT_ENGINE_MODE = 0, BK_OPT_SLAB_LAG = 1, BK_OPT_SPLIT_W2 = 2, BK_OPT_E_SOURCE = 3 };
 int bk_set_option(bk_ctx* ctx, int option, int64_t value);
 int bk_get_option(const bk_ctx* ctx, int option, int64_t* value);
 

@@ -70,4 +70,24 @@ def test_tuner_sweeps_and_caches(eng, tmp_path):
     assert tune.apply(eng, 20, bk.BK_C64, cache_path=path) == e["best"]
     assert eng.get_option("engine_mode") == e["best"]["engine_mode"]
     for k in tune.KNOBS:
-        eng.set_option(k, {"engine_mode": 0, "slab_lag": 3, "split_w2": 0}[k])
+        eng.set_option(k, tune.DEFAULTS[k])
+
+
+@pytest.mark.parametrize("n,precision", [(22, bk.BK_C64), (21, bk.BK_C128)])
+def test_recomputed_energies_equal_the_table(eng, n, precision):
+    """E(s) from popcounts in the pass (BK_OPT_E_SOURCE = 1) is the same integer as
+    the table's: identical series in both schedules."""
+    bits, e0 = bk.select_trap(n, 4, 200, 0.05)
+    steps = 12
+    ref = None
+    for mode in (0, 1):
+        for src in (0, 1):
+            eng.set_option("engine_mode", mode)
+            eng.set_option("e_source", src)
+            out = eng.evolve(n, bits, 0.35, 0.02, steps, measure=range(0, steps + 1, 3), e0=e0, precision=precision)
+            if ref is None:
+                ref = out
+            for a, b in zip(ref, out):
+                assert np.array_equal(a, b)
+    eng.set_option("engine_mode", 0)
+    eng.set_option("e_source", 0)
