@@ -148,6 +148,23 @@ def cpu_baseline(n, steps, g, dt):
                       f"mean step time {np.mean(secs):.3f} s"}
 
 
+def ed_baseline(sizes=(8, 10, 12), g=0.35, points=41, dt=0.5):
+    """The reference's CPU fallback for small N (dense exact diagonalisation,
+    connector.cuh:683-805 on Eigen, absent here) restated with numpy/LAPACK
+    (oracle/ed_oracle.py): eigh of the 2^N x 2^N Hamiltonian and `points`
+    propagated time points, timed on the host's cores."""
+    from oracle import oracle as O
+    from oracle import ed_oracle
+    out = {}
+    for n in sizes:
+        bits = int(O.steepest_descent(n, 12345 % (1 << n))[0])
+        e0 = O.labs_energy(n, bits)
+        t0 = time.perf_counter()
+        ed_oracle.propagate(n, g, bits, e0, np.arange(points) * dt, O.energy_table(n))
+        out[str(n)] = {"seconds": time.perf_counter() - t0, "time_points": points}
+    return {"kind": "numpy/LAPACK restatement (Eigen absent)", "cores": os.cpu_count(), "sizes": out}
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -485,6 +502,7 @@ def main():
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(n, a.cpu_baseline_steps, a.g, a.dt)
+            line["cpu_baseline"]["ed_dense"] = ed_baseline()
         except Exception as exc:  # report, do not hide
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                     "sample": f"failed: {exc}"}

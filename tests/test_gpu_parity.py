@@ -157,3 +157,32 @@ def test_host_side_errors(eng):
     # the context stays usable after rejected calls
     p, _, _ = eng.evolve(10, 0, 0.35, 0.05, 2)
     assert len(p) == 3
+
+
+def test_c64_state_infidelity_n24_config(eng):
+    """complex64 against complex128 at the N = 24 configuration (1000 steps):
+    state infidelity 1 - |<psi_64|psi_128>|^2 of the exported statevectors."""
+    bits = 0xFAD33
+    eng.evolve(24, bits, 0.35, 0.02, 1000, measure=[1000], precision=bk.BK_C64)
+    s64 = eng.export_state(24)
+    eng.evolve(24, bits, 0.35, 0.02, 1000, measure=[1000], precision=bk.BK_C128)
+    s128 = eng.export_state(24)
+    ov = np.vdot(s64, s128) / (np.linalg.norm(s64) * np.linalg.norm(s128))
+    infidelity = 1.0 - abs(ov) ** 2
+    assert infidelity <= 1e-8, infidelity
+
+
+def test_plain_config_n12_against_oracle_and_ed(eng):
+    """The N = 12 configuration: complex128, dt = 0.05, 400 steps (T = 20), P_< and
+    <d_H> every 10 steps; equal to the oracle to 1e-10 and to dense exact
+    diagonalisation (4096 x 4096) within the O(dt^2) Trotter error."""
+    from oracle import ed_oracle
+    n, dt, steps = 12, 0.05, 400
+    bits, e0 = bk.select_trap(n, 42, 1000, 0.05)
+    meas = range(0, steps + 1, 10)
+    p, d, nn = eng.evolve(n, bits, 0.35, dt, steps, measure=meas, e0=e0, precision=bk.BK_C128)
+    po, do, _ = O.trotter_evolve(n, bits, e0, 0.35, dt, steps, measure=meas)
+    assert np.max(np.abs(p - po)) <= 1e-10 and np.max(np.abs(d - do)) <= 1e-10 * n
+    pe, de = ed_oracle.propagate(n, 0.35, bits, e0, np.arange(0, steps + 1, 10) * dt, O.energy_table(n))
+    assert np.max(np.abs(p - pe)) <= 5e-3
+    assert np.max(np.abs(d - de)) <= 5e-3 * n
