@@ -456,4 +456,16 @@ __global__ void __launch_bounds__(32 * kDescentWarps)
   }
 }
 
+// Per-shot energy and Hamming distance to the start state for drawn basis
+// states (the reference evaluates both on the host for every shot,
+// src/sampling/sampler.cuh:575-596): one thread per shot, exact integers.
+__global__ void shot_stats_kernel(const unsigned long long* __restrict__ states, long long count, int n,
+                                  unsigned long long s0, int* __restrict__ energies, int* __restrict__ flips) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const unsigned long long b = states[i];
+  energies[i] = labs_energy((uint32_t)b, n);
+  flips[i] = __popcll(b ^ s0);
+}
+
 }  // namespace bk

@@ -2281,7 +2281,26 @@ int bk_sampler_run(bk_ctx* c, const bk_sampler_config* cfg, uint64_t start_bits,
   std::vector<double> pl(times.size()), dh(times.size());
   BK_TRY(bk_evolve(c, &ep, pl.data(), dh.data(), nullptr));
 
-  // ---- per-shot statistics (sampler.cuh:575-597)
+  // ---- per-shot energy and Hamming distance on the device (the drawn states are
+  // still there), statistics on the host (sampler.cuh:575-597)
+  const size_t n_draws = drawn.size();
+  std::vector<int> shot_e(n_draws), shot_d(n_draws);
+  if (n_draws > 0) {
+    void* scratch = nullptr;
+    BK_CUDA(c, cudaMallocAsync(&scratch, n_draws * 2 * sizeof(int), c->stream));
+    int* d_e = static_cast<int*>(scratch);
+    int* d_f = d_e + n_draws;
+    shot_stats_kernel<<<(unsigned)((n_draws + 255) / 256), 256, 0, c->stream>>>(
+        c->d_samples, (long long)n_draws, n, (unsigned long long)(start_bits & ((1ull << n) - 1ull)), d_e, d_f);
+    const cudaError_t le = cudaGetLastError();
+    cudaError_t ce = cudaMemcpyAsync(shot_e.data(), d_e, n_draws * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(shot_d.data(), d_f, n_draws * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(scratch, c->stream);
+    BK_CUDA(c, le);
+    BK_CUDA(c, ce);
+    BK_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   std::vector<bk_seed_stats> ss((size_t)n_seeds);
   for (int s = 0; s < n_seeds; ++s) {
     std::memset(&ss[(size_t)s], 0, sizeof(bk_seed_stats));
@@ -2294,12 +2313,13 @@ int bk_sampler_run(bk_ctx* c, const bk_sampler_config* cfg, uint64_t start_bits,
     for (int s = 0; s < n_seeds; ++s) {
       uint64_t flips = 0;
       for (int i = 0; i < shots; ++i) {
-        const uint64_t b = drawn[pt * per_point + (size_t)s * shots + (size_t)i];
+        const size_t k = pt * per_point + (size_t)s * shots + (size_t)i;
+        const uint64_t b = drawn[k];
         uniq.insert(b);
-        const int d = __builtin_popcountll(start_bits ^ b);
+        const int d = shot_d[k];
         flips += (uint64_t)d;
         if (s == 0) flips_primary += (uint64_t)d;
-        const int64_t e = host_energy(n, b);
+        const int64_t e = shot_e[k];
         if (e < ss[(size_t)s].best_energy) ss[(size_t)s].best_energy = e;
         if (e < E0) {
           ss[(size_t)s].improved_shots++;
