@@ -7,7 +7,9 @@ Knobs (engine options, include/bk_engine.h):
   slab_lag     persistent engine: slabs between a slab's A1 and S2 tasks;
   split_w2     qubits of the S2 pass (the rest go to S3), 0 = engine default;
   e_source     E(s) for the diagonal phase: 0 = uint16 table, 1 = recomputed
-               from popcounts in the pass (no E traffic, more arithmetic).
+               from popcounts in the pass (no E traffic, more arithmetic);
+  a1_wide      per-pass schedule: the A1 pass with 512 threads x 8 elements
+               (1) or 256 x 16 (0).
 For the batched engine the knob is the task-block lag between a statevector
 slab's A1 and S2 tasks.
 
@@ -26,8 +28,8 @@ import os
 from ._lib import BK_C64, BK_C128
 
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.json")
-KNOBS = ("engine_mode", "slab_lag", "split_w2", "e_source")
-DEFAULTS = {"engine_mode": 0, "slab_lag": 3, "split_w2": 0, "e_source": 0}
+KNOBS = ("engine_mode", "slab_lag", "split_w2", "e_source", "a1_wide")
+DEFAULTS = {"engine_mode": 0, "slab_lag": 3, "split_w2": 0, "e_source": 0, "a1_wide": 0}
 ELEM_BITS = 12  # element bits of one 64 KB tile
 
 
@@ -55,12 +57,13 @@ def candidates(n, precision):
     widths = [0] + [w for w in (d - 1, d + 1) if 1 <= w <= 9 and w <= rest and rest - w <= 9]
     out = []
     for w in widths:
-        out.append(dict(engine_mode=1, slab_lag=3, split_w2=w, e_source=0))
+        for wide in (0, 1):
+            out.append(dict(engine_mode=1, slab_lag=3, split_w2=w, e_source=0, a1_wide=wide))
         for lag in (1, 2, 3, 4, 6):
-            out.append(dict(engine_mode=0, slab_lag=lag, split_w2=w, e_source=0))
+            out.append(dict(engine_mode=0, slab_lag=lag, split_w2=w, e_source=0, a1_wide=0))
     # E recomputed in the pass, on the default split of both schedules
-    out.append(dict(engine_mode=1, slab_lag=3, split_w2=0, e_source=1))
-    out.append(dict(engine_mode=0, slab_lag=3, split_w2=0, e_source=1))
+    out.append(dict(engine_mode=1, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))
+    out.append(dict(engine_mode=0, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))
     return out
 
 

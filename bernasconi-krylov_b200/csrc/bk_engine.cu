@@ -92,6 +92,7 @@ struct bk_ctx {
   int engine_mode = 0;        // 0 persistent dataflow, 1 one launch per pass (tile grid)
   int force_w2 = 0;           // S2 width when > 0 and valid for the size (else the default split)
   int e_recompute = 0;        // tile engine: 1 = E(s) recomputed from popcounts in A1, 0 = uint16 table
+  int a1_wide = 0;            // per-pass schedule: 1 = A1 with 512 threads x 8 elements
   std::map<int, uint16_t*> batch_E;  // E tables of batched runs, per n
   void* d_batch_state = nullptr;
   size_t batch_state_cap = 0;
@@ -786,6 +787,7 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
   if (c->engine_mode == 1) {
     // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_pass_kernel<R>), PersistSmem::kBytes));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_wide_kernel<R>), PersistSmem::kBytes));
     using SampT = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
     BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &D, sizeof(D), cudaMemcpyHostToDevice, st));
     BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
@@ -804,7 +806,10 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
         break;
       }
       BK_TRY(ev_begin(c, "tile_a1", &ev));
-      tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_A1, (uint32_t)k, err);
+      if (c->a1_wide)
+        tile_a1_wide_kernel<R><<<n_a1, kA1WideThreads, PersistSmem::kBytes, st>>>(D, (uint32_t)k, err);
+      else
+        tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_A1, (uint32_t)k, err);
       BK_CUDA(c, cudaGetLastError());
       BK_TRY(ev_end(c, ev));
       BK_TRY(ev_begin(c, "tile_s2", &ev));
@@ -1914,6 +1919,10 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
       if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "E source %lld", (long long)value);
       c->e_recompute = (int)value;
       return BK_OK;
+    case BK_OPT_A1_WIDE:
+      if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "A1 width %lld", (long long)value);
+      c->a1_wide = (int)value;
+      return BK_OK;
     default:
       return fail(c, BK_ERR_INVALID, "unknown option %d", option);
   }
@@ -1926,6 +1935,7 @@ int bk_get_option(const bk_ctx* c, int option, int64_t* value) {
     case BK_OPT_SLAB_LAG: *value = c->slab_lag; return BK_OK;
     case BK_OPT_SPLIT_W2: *value = c->force_w2; return BK_OK;
     case BK_OPT_E_SOURCE: *value = c->e_recompute; return BK_OK;
+    case BK_OPT_A1_WIDE: *value = c->a1_wide; return BK_OK;
     default: return BK_ERR_INVALID;
   }
 }

@@ -391,24 +391,25 @@ __device__ __forceinline__ uint32_t load_e(const unsigned char* etile, uint32_t 
 }
 
 // consumer-side block reduction: per-tile partials, last tile of the step
-// reduces all of them in index order into results[slot]
+// reduces all of them in index order into results[slot]; NW warps per CTA
+template <int NW = kComputeThreads / 32>
 __device__ __forceinline__ void compute_reduce(MeasureAcc acc, double* partials, unsigned int* ticket,
                                                double* results, int slot, uint32_t tile, uint32_t ntiles,
-                                               double* red /* smem [3][8] */, int* last_flag) {
+                                               double* red /* smem [3][NW] */, int* last_flag) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double a = warp_sum(acc.norm), b = warp_sum(acc.p_less), c = warp_sum(acc.d_h);
   if (lane == 0) {
-    red[0 * 8 + warp] = a;
-    red[1 * 8 + warp] = b;
-    red[2 * 8 + warp] = c;
+    red[0 * NW + warp] = a;
+    red[1 * NW + warp] = b;
+    red[2 * NW + warp] = c;
   }
-  compute_sync();
+  __syncthreads();
   if (tid == 0) {
     double s0 = 0, s1 = 0, s2 = 0;
-    for (int w = 0; w < 8; ++w) {
+    for (int w = 0; w < NW; ++w) {
       s0 += red[w];
-      s1 += red[8 + w];
-      s2 += red[16 + w];
+      s1 += red[NW + w];
+      s2 += red[2 * NW + w];
     }
     partials[3 * (size_t)tile + 0] = s0;
     partials[3 * (size_t)tile + 1] = s1;
@@ -416,11 +417,11 @@ __device__ __forceinline__ void compute_reduce(MeasureAcc acc, double* partials,
     __threadfence();
     *last_flag = (atomicAdd(ticket, 1u) == ntiles - 1u);
   }
-  compute_sync();
+  __syncthreads();
   if (!*last_flag) return;
   __threadfence();
   double s0 = 0, s1 = 0, s2 = 0;
-  for (uint32_t i = tid; i < ntiles; i += kComputeThreads) {
+  for (uint32_t i = tid; i < ntiles; i += 32u * NW) {
     s0 += __ldcg(&partials[3 * (size_t)i + 0]);
     s1 += __ldcg(&partials[3 * (size_t)i + 1]);
     s2 += __ldcg(&partials[3 * (size_t)i + 2]);
@@ -428,19 +429,19 @@ __device__ __forceinline__ void compute_reduce(MeasureAcc acc, double* partials,
   s0 = warp_sum(s0);
   s1 = warp_sum(s1);
   s2 = warp_sum(s2);
-  compute_sync();
+  __syncthreads();
   if (lane == 0) {
     red[warp] = s0;
-    red[8 + warp] = s1;
-    red[16 + warp] = s2;
+    red[NW + warp] = s1;
+    red[2 * NW + warp] = s2;
   }
-  compute_sync();
+  __syncthreads();
   if (tid == 0) {
     double nn = 0, p = 0, d = 0;
-    for (int w = 0; w < 8; ++w) {
+    for (int w = 0; w < NW; ++w) {
       nn += red[w];
-      p += red[8 + w];
-      d += red[16 + w];
+      p += red[NW + w];
+      d += red[2 * NW + w];
     }
     results[4 * (size_t)slot + 0] = p;
     results[4 * (size_t)slot + 1] = d;
@@ -584,7 +585,7 @@ struct PersistSmem {
   static constexpr int kStageBytes = kStageTileBytes + kStageEBytes;
   static constexpr int kPhaseOff = kStageBytes;
   static constexpr int kRedOff = kPhaseOff + 3328;  // >= both phase table footprints
-  static constexpr int kBytes = kRedOff + 256;
+  static constexpr int kBytes = kRedOff + 512;  // reduction scratch: [3][16] doubles
 };
 
 template <class R>
@@ -812,6 +813,122 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
   }
   // a load still in flight (issued early for a task that will not run) lands before exit
   if (tid == 0 && inflight) mbar_wait_bounded(fb, phase, P.err);
+}
+
+// ---------------------------------------------------------------------------
+// Wide A1 for the per-pass schedule: 512 threads x 8 elements per tile, so 32
+// warps share an SM (two CTAs) instead of 16 — more latency hiding for the
+// diagonal phase, the pass's dominant cost. Four rounds of 3 register bits
+// (tile bits 3-5 in the TMA layout, then 0-2, 6-8, 9-11 through the swizzled
+// shared tile; every 16-byte access conflict free, the last round's stores
+// 512 contiguous bytes per warp). Same arithmetic per element as process_a1.
+// ---------------------------------------------------------------------------
+struct PlanA1Wide {
+  static constexpr uint32_t R1_REG = 0x038, R1_LANE = 0x0C7, R1_WARP = 0xF00;
+  static constexpr uint32_t R2_REG = 0x007, R2_LANE = 0x0F8, R2_WARP = 0xF00;
+  static constexpr uint32_t R3_REG = 0x1C0, R3_LANE = 0x01F, R3_WARP = 0xE20;
+  static constexpr uint32_t R4_REG = 0xE00, R4_LANE = 0x01F, R4_WARP = 0x1E0;
+};
+constexpr int kA1WideThreads = 512;
+
+template <class R, uint32_t REG, bool SWZ>
+__device__ __forceinline__ void el8_load(const unsigned char* s, typename El<R>::T (&v)[8], uint32_t base) {
+  const uint32_t sb = SWZ ? swz<double>(base) : base;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t o = SWZ ? swz<double>(pdep((uint32_t)j, REG)) : pdep((uint32_t)j, REG);
+    v[j] = El<R>::ld(s + 16u * (sb ^ o));
+  }
+}
+template <class R, uint32_t REG>
+__device__ __forceinline__ void el8_store_swz(unsigned char* s, const typename El<R>::T (&v)[8], uint32_t base) {
+  const uint32_t sb = swz<double>(base);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) El<R>::st(s + 16u * (sb ^ swz<double>(pdep((uint32_t)j, REG))), v[j]);
+}
+template <class R>
+__device__ __forceinline__ void el8_bflys(typename El<R>::T (&v)[8], R t) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (!(j & (1 << k))) El<R>::bfly(v[j], v[j | (1 << k)], t);
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kA1WideThreads, 2)
+    tile_a1_wide_kernel(const __grid_constant__ InstDesc<R> D, uint32_t step, int* err) {
+  using PL = PlanA1Wide;
+  using E = El<R>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full_bar;
+  __shared__ int last_flag;
+  unsigned char* tile = smem;
+  const unsigned char* etile = smem + kStageTileBytes;
+  unsigned char* phase_smem = smem + PersistSmem::kPhaseOff;
+  double* red = reinterpret_cast<double*>(smem + PersistSmem::kRedOff);
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t fb = smem_addr(&full_bar);
+  const uint32_t t_idx = blockIdx.x;
+  const uint32_t tile_base = t_idx << kElemBits;
+  StageMeta m;
+  m.kind = TASK_A1;
+  m.inst = 0;
+  m.tile = t_idx;
+  m.step = step;
+  if (tid == 0) {
+    mbar_init(fb, 1);
+    fence_barrier_init();
+    issue_task_load(D, m, tile, fb);
+  }
+  PhaseV<R>::stage(D.phase, phase_smem, (int)tid, kA1WideThreads);
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(fb, 0, err);
+  if (__syncthreads_or(!ok)) return;
+  typename E::T v[8];
+  const R t = D.tan[step];
+  const int slot = D.slot[step];
+  MeasureAcc acc;
+  const uint32_t b1 = pdep(lane, PL::R1_LANE) | pdep(warp, PL::R1_WARP);
+  el8_load<R, PL::R1_REG, false>(tile, v, b1);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t i = b1 | pdep((uint32_t)j, PL::R1_REG);
+    const uint32_t e = D.e_recompute ? recompute_e<R>(tile_base | i, D.n) : load_e<R>(etile, i);
+    if (slot >= 0) measure_el(acc, v[j], e, tile_base | i, D.e0, D.s0);
+    PhaseV<R>::apply(v[j], e, D.phase, phase_smem, false);
+    E::bfly_inner(v[j], t);
+  }
+  const R sc = D.scale[step];
+  if (sc != (R)1) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) E::scale(v[j], sc);
+  }
+  el8_bflys<R>(v, t);
+  __syncthreads();
+  el8_store_swz<R, PL::R1_REG>(tile, v, b1);
+  __syncthreads();
+  const uint32_t b2 = pdep(lane, PL::R2_LANE) | pdep(warp, PL::R2_WARP);
+  el8_load<R, PL::R2_REG, true>(tile, v, b2);
+  el8_bflys<R>(v, t);
+  __syncthreads();
+  el8_store_swz<R, PL::R2_REG>(tile, v, b2);
+  __syncthreads();
+  const uint32_t b3 = pdep(lane, PL::R3_LANE) | pdep(warp, PL::R3_WARP);
+  el8_load<R, PL::R3_REG, true>(tile, v, b3);
+  el8_bflys<R>(v, t);
+  __syncthreads();
+  el8_store_swz<R, PL::R3_REG>(tile, v, b3);
+  __syncthreads();
+  const uint32_t b4 = pdep(lane, PL::R4_LANE) | pdep(warp, PL::R4_WARP);
+  el8_load<R, PL::R4_REG, true>(tile, v, b4);
+  el8_bflys<R>(v, t);
+  const uint64_t pol = policy_evict_last();
+#pragma unroll
+  for (int j = 0; j < 8; ++j) E::stg(D.state + 16ull * (tile_base | b4 | pdep((uint32_t)j, PL::R4_REG)), v[j], pol);
+  if (slot >= 0)
+    compute_reduce<kA1WideThreads / 32>(acc, D.partials, D.ticket, D.results, slot, t_idx, D.n_a1, red, &last_flag);
 }
 
 // ---------------------------------------------------------------------------

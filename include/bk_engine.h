@@ -272,8 +272,10 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       0 = the engine's default split; a width that does not fit a size is ignored;
  *   BK_OPT_E_SOURCE: where the diagonal phase and P_< get E(s): 0 = the cached
  *       uint16 table (read with the A1 tile), 1 = recomputed in the pass from the
- *       popcount form C_k = (n-k) - 2 popcount((x ^ (x >> k)) & (2^(n-k) - 1)). */
-enum { BK_OPT_ENGINE_MODE = 0, BK_OPT_SLAB_LAG = 1, BK_OPT_SPLIT_W2 = 2, BK_OPT_E_SOURCE = 3 };
+ *       popcount form C_k = (n-k) - 2 popcount((x ^ (x >> k)) & (2^(n-k) - 1));
+ *   BK_OPT_A1_WIDE: per-pass schedule (mode 1), 1 = the A1 pass with 512 threads
+ *       of 8 elements (more warps per SM for the diagonal phase), 0 = 256 x 16. */
+enum { BK_OPT_ENGINE_MODE = 0, BK_OPT_SLAB_LAG = 1, BK_OPT_SPLIT_W2 = 2, BK_OPT_E_SOURCE = 3, BK_OPT_A1_WIDE = 4 };
 int bk_set_option(bk_ctx* ctx, int option, int64_t value);
 int bk_get_option(const bk_ctx* ctx, int option, int64_t* value);
 

@@ -91,3 +91,25 @@ def test_recomputed_energies_equal_the_table(eng, n, precision):
                 assert np.array_equal(a, b)
     eng.set_option("engine_mode", 0)
     eng.set_option("e_source", 0)
+
+
+def test_wide_a1_matches_oracle_c128(eng):
+    """The 512-thread A1 of the per-pass schedule (BK_OPT_A1_WIDE): complex128
+    series within 1e-10 of the oracle; complex64 within 1e-6 of the 256-thread A1
+    (the same rotations in another round order)."""
+    n, steps = 17, 24
+    bits, e0 = bk.select_trap(n, 6, 200, 0.05)
+    eng.set_option("engine_mode", 1)
+    eng.set_option("a1_wide", 1)
+    try:
+        p, d, nn = eng.evolve(n, bits, 0.35, 0.05, steps, e0=e0, precision=bk.BK_C128)
+        po, do, _ = O.trotter_evolve(n, bits, e0, 0.35, 0.05, steps)
+        assert np.max(np.abs(p - po)) <= 1e-10 and np.max(np.abs(d - do)) <= 1e-10 * n
+        b2, e2 = bk.select_trap(22, 6, 200, 0.05)
+        pw, dw, _ = eng.evolve(22, b2, 0.35, 0.02, 40, measure=range(0, 41, 5), e0=e2, precision=bk.BK_C64)
+        eng.set_option("a1_wide", 0)
+        ps, ds, _ = eng.evolve(22, b2, 0.35, 0.02, 40, measure=range(0, 41, 5), e0=e2, precision=bk.BK_C64)
+        assert np.max(np.abs(pw - ps)) <= 1e-6 and np.max(np.abs(dw - ds)) <= 1e-6 * 22
+    finally:
+        eng.set_option("a1_wide", 0)
+        eng.set_option("engine_mode", 0)

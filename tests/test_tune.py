@@ -11,6 +11,7 @@ def test_candidates_cover_modes_lags_and_valid_splits():
     assert {x["split_w2"] for x in c} == {0, 7, 9}
     assert {x["slab_lag"] for x in c if x["engine_mode"] == 0} == {1, 2, 3, 4, 6}
     assert {x["e_source"] for x in c} == {0, 1}
+    assert {x["a1_wide"] for x in c if x["engine_mode"] == 1} == {0, 1}
     for n, prec in ((30, bk.BK_C64), (30, bk.BK_C128), (22, bk.BK_C64), (14, bk.BK_C64)):
         rest = (n - 1 if prec == bk.BK_C64 else n) - tune.ELEM_BITS
         for x in tune.candidates(n, prec):
