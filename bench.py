@@ -449,8 +449,7 @@ def main():
     # algorithmic bytes per launch: a pass reads and writes the state once (2 S per
     # amplitude); one persistent launch runs all T Trotter steps of a call (4 S per
     # amplitude-step: two such passes per step)
-    per_launch_bytes = {"a1_step": 2 * S, "a1_step_measure": 2 * S, "a1_measure": S, "measure": S,
-                        "plain_phase": 2 * S, "plain_rx": 2 * S, "persist": 4 * S * T,
+    per_launch_bytes = {"measure": S, "plain_phase": 2 * S, "plain_rx": 2 * S, "persist": 4 * S * T,
                         "tile_a1": 2 * S, "tile_s2": 2 * S, "tile_s3": 2 * S, "tile_m": S}
     dom = max(timing.items(), key=lambda kv: kv[1][1])
     dname, (dl, dms) = dom

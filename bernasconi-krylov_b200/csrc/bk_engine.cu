@@ -108,8 +108,6 @@ struct bk_ctx {
   size_t adj_cap = 0;
   void* d_descent = nullptr;  // batched steepest descent: starts, final states, energies, evaluations
   size_t descent_cap = 0;
-  // tensor maps, keyed by (state ptr, n, precision, pass)
-  std::map<std::string, TmaDesc> tma;
   // last evolution (for export / sampling)
   bool have_state = false;
   bool last_planar = false;
@@ -308,7 +306,6 @@ int ensure_energy(bk_ctx* c, int n) {
   if (c->d_E) cudaFree(c->d_E);
   c->d_E = nullptr;
   c->e_n = -1;
-  c->tma.clear();
   const size_t count = 1ull << n;
   BK_CUDA(c, cudaMalloc(&c->d_E, std::max<size_t>(count, 8) * sizeof(uint16_t)));
   const uint32_t threads = 256, per = (uint32_t)((count + 7) / 8);
@@ -324,7 +321,6 @@ int ensure_state(bk_ctx* c, int n, int prec) {
   if (c->d_state) cudaFree(c->d_state);
   c->d_state = nullptr;
   c->state_bytes = 0;
-  c->tma.clear();
   BK_CUDA(c, cudaMalloc(&c->d_state, bytes));
   c->state_bytes = bytes;
   c->st_n = n;
@@ -776,22 +772,18 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
   BK_TRY(persist_prepare<R>(c, p, S, angle_unit, tans, scales, &run));
   const int n = p->n;
   cudaStream_t st = c->stream;
-  char* base = run.base;
   unsigned int* ctr = run.ctr;
   const uint32_t slabs = run.slabs;
   int* err = run.err;
   const uint32_t n_a1 = run.n_a1, n_s2 = run.n_s2, n_s3 = run.n_s3;
-  const size_t o_desc = run.o_desc;
-  InstDesc<R> D = run.D;
+  const InstDesc<R> D = run.D;
 
   if (c->engine_mode == 1) {
     // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_pass_kernel<R>), PersistSmem::kBytes));
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_wide_kernel<R>), PersistSmem::kBytes));
     using SampT = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
-    BK_CUDA(c, cudaMemcpyAsync(base + o_desc, &D, sizeof(D), cudaMemcpyHostToDevice, st));
     BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
-    const InstDesc<R>* dd = reinterpret_cast<const InstDesc<R>*>(base + o_desc);
     for (int k = 0; k <= p->n_steps; ++k) {
       if (S.sample_pt[(size_t)k] >= 0)
         BK_TRY(launch_sampling_t(c, reinterpret_cast<const SampT*>(c->d_state), n, S.sample_pt[(size_t)k], S.shots));
@@ -2124,7 +2116,6 @@ int bk_adjoint(bk_ctx* c, const bk_adjoint_params* p, double* value_out, double*
   const int n_ckpt = n_ck(K);
   BK_TRY(ensure_buffer(c, &c->d_lam, &c->lam_cap, sbytes));
   if (n_ckpt > 0) BK_TRY(ensure_buffer(c, &c->d_ckpt, &c->ckpt_cap, sbytes * (size_t)n_ckpt));
-  c->tma.clear();
   std::vector<double> gs;
   if (p->precision == BK_C64)
     BK_TRY(adjoint_t<float>(c, p, g_step, e0, angle_unit, K, n_ckpt, value_out, &gs, stats));
