@@ -193,10 +193,10 @@ __device__ __forceinline__ double adj_a1(unsigned char* sp, unsigned char* sl, c
   m += popc_c(PL::A1_R1_REG);
   el_bflys<R, PL::A1_R1_REG, PL::A1_R1_REG>(v, t);
   el_bflys<R, PL::A1_R1_REG, PL::A1_R1_REG>(u, t);
-  __syncthreads();
+  warp_sync();  // round-1 reads vs swizzled stores: same warp
   el_store_swz<R, PL::A1_R1_REG>(sp, v, b1);
   el_store_swz<R, PL::A1_R1_REG>(sl, u, b1);
-  __syncthreads();
+  warp_sync();  // rounds 1 and 2 share the warp bits
   const uint32_t b2 = pdep(lane, PL::A1_R2_LANE) | pdep(warp, PL::A1_R2_WARP);
   el_load<R, PL::A1_R2_REG, true>(sp, v, b2);
   el_load<R, PL::A1_R2_REG, true>(sl, u, b2);
@@ -205,8 +205,7 @@ __device__ __forceinline__ double adj_a1(unsigned char* sp, unsigned char* sl, c
   m += popc_c(PL::A1_R2_REG);
   el_bflys<R, PL::A1_R2_REG, PL::A1_R2_REG>(v, t);
   el_bflys<R, PL::A1_R2_REG, PL::A1_R2_REG>(u, t);
-  __syncthreads();
-  el_store_swz<R, PL::A1_R2_REG>(sp, v, b2);
+  el_store_swz<R, PL::A1_R2_REG>(sp, v, b2);  // in place
   el_store_swz<R, PL::A1_R2_REG>(sl, u, b2);
   __syncthreads();
   const uint32_t b3 = pdep(lane, PL::A1_R3_LANE) | pdep(warp, PL::A1_R3_WARP);
@@ -256,7 +255,7 @@ __device__ __forceinline__ double adj_s(unsigned char* sp, unsigned char* sl, co
     el_gstore_plain<R, PL::S_R1_REG, CP>(D.lam, u, tile_base, b1, h0);
   } else {
     using R2 = StridedR2<double, W>;
-    __syncthreads();
+    warp_sync();  // round-1 reads vs swizzled stores: same warp
     el_store_swz<R, PL::S_R1_REG>(sp, v, b1);
     el_store_swz<R, PL::S_R1_REG>(sl, u, b1);
     __syncthreads();

@@ -300,6 +300,15 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void compute_sync() { __syncthreads(); }
+// Barriers between the rounds of a tile: a round's layout change only moves
+// data inside a warp (round 1 -> 2 of A1, the swizzled store after an
+// unswizzled read) or inside a warp pair (512-thread A1, round 2 -> 3); a store
+// back into the slots the same thread has just read needs no barrier.
+__device__ __forceinline__ void warp_sync() { __syncwarp(); }
+// warps 2m and 2m + 1 (named barrier 1 + m, 64 threads; at most 16 warps)
+__device__ __forceinline__ void pair_sync() {
+  asm volatile("bar.sync %0, 64;" ::"r"(1u + (threadIdx.x >> 6)) : "memory");
+}
 __device__ __forceinline__ bool aborted(const int* abort) {
   return *reinterpret_cast<const volatile int*>(abort) != 0;
 }
@@ -498,14 +507,13 @@ __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned c
       for (int j = 0; j < 16; ++j) E::scale(v[j], sc);
     }
     el_bflys<R, PL::A1_R1_REG, PL::A1_R1_REG>(v, t);
-    compute_sync();
+    warp_sync();  // round-1 reads vs swizzled stores: same warp (warp bits 9-11)
     el_store_swz<R, PL::A1_R1_REG>(tile, v, b1);
-    compute_sync();
+    warp_sync();  // rounds 1 and 2 share the warp bits
     const uint32_t b2 = pdep(lane, PL::A1_R2_LANE) | pdep(warp, PL::A1_R2_WARP);
     el_load<R, PL::A1_R2_REG, true>(tile, v, b2);
     el_bflys<R, PL::A1_R2_REG, PL::A1_R2_REG>(v, t);
-    compute_sync();
-    el_store_swz<R, PL::A1_R2_REG>(tile, v, b2);
+    el_store_swz<R, PL::A1_R2_REG>(tile, v, b2);  // in place
     compute_sync();
     const uint32_t b3 = pdep(lane, PL::A1_R3_LANE) | pdep(warp, PL::A1_R3_WARP);
     el_load<R, PL::A1_R3_REG, true>(tile, v, b3);
@@ -540,7 +548,7 @@ __device__ __forceinline__ void process_s(unsigned char* tile, unsigned char* st
     el_gstore<R, PL::S_R1_REG, CP>(state, v, tile_base, b1, h0, policy_evict_first());
   } else {
     using R2 = StridedR2<double, W>;
-    compute_sync();
+    warp_sync();  // round-1 reads vs swizzled stores: same warp
     el_store_swz<R, PL::S_R1_REG>(tile, v, b1);
     compute_sync();
     const uint32_t b2 = pdep(lane, R2::LANE) | pdep(warp, R2::WARP);
@@ -906,20 +914,18 @@ __global__ void __launch_bounds__(kA1WideThreads, 2)
     for (int j = 0; j < 8; ++j) E::scale(v[j], sc);
   }
   el8_bflys<R>(v, t);
-  __syncthreads();
+  warp_sync();  // round-1 reads vs swizzled stores: same warp
   el8_store_swz<R, PL::R1_REG>(tile, v, b1);
-  __syncthreads();
+  warp_sync();  // rounds 1 and 2 share the warp bits (8-11)
   const uint32_t b2 = pdep(lane, PL::R2_LANE) | pdep(warp, PL::R2_WARP);
   el8_load<R, PL::R2_REG, true>(tile, v, b2);
   el8_bflys<R>(v, t);
-  __syncthreads();
-  el8_store_swz<R, PL::R2_REG>(tile, v, b2);
-  __syncthreads();
+  el8_store_swz<R, PL::R2_REG>(tile, v, b2);  // in place
+  pair_sync();  // rounds 2 and 3 share warp bits 9-11: data moves inside a warp pair
   const uint32_t b3 = pdep(lane, PL::R3_LANE) | pdep(warp, PL::R3_WARP);
   el8_load<R, PL::R3_REG, true>(tile, v, b3);
   el8_bflys<R>(v, t);
-  __syncthreads();
-  el8_store_swz<R, PL::R3_REG>(tile, v, b3);
+  el8_store_swz<R, PL::R3_REG>(tile, v, b3);  // in place
   __syncthreads();
   const uint32_t b4 = pdep(lane, PL::R4_LANE) | pdep(warp, PL::R4_WARP);
   el8_load<R, PL::R4_REG, true>(tile, v, b4);
