@@ -59,6 +59,8 @@ def parse():
                     help="large: the N=28 headline; batched: 512 instances (64 traps x 8 g), N in {16,18,20,22}")
     ap.add_argument("--slab-lag", type=int, default=None)
     ap.add_argument("--split-w2", type=int, default=None, help="qubits of the S2 pass (0 = default split)")
+    ap.add_argument("--a1-kernel", type=int, default=None, choices=[0, 1, 2],
+                    help="per-pass A1 kernel: 0 = 256x16, 1 = 512x8, 2 = warp-local (element bits 0-8)")
     ap.add_argument("--no-tune", action="store_true", help="engine defaults instead of the autotuner's choice")
     return ap.parse_args()
 
@@ -67,9 +69,9 @@ def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except Exception:
-        return 6650.0, "fallback"
+        return 6650.0, "fallback (6650 GB/s copy bandwidth; MEASURED_PEAKS.json absent)"
 
 
 def committed_traffic():
@@ -221,7 +223,7 @@ def tuned_knobs(eng, a, n, prec, trap):
     for this device and size, else a tuning sweep now (not timed, not cached)."""
     from bk_b200 import tune
     explicit = {k: v for k, v in (("engine_mode", a.engine_mode), ("slab_lag", a.slab_lag),
-                                  ("split_w2", a.split_w2)) if v is not None}
+                                  ("split_w2", a.split_w2), ("a1_wide", a.a1_kernel)) if v is not None}
     if explicit or a.no_tune:
         for k, v in explicit.items():
             eng.set_option(k, v)
@@ -470,7 +472,7 @@ def main():
                        "l2": f"state {((1 << n) * S) / 2**30:.1f} GiB > 126 MB L2, no flush needed",
                        "parallelism": f"replicas x{world}", "tuning": tuning},
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "frac": achieved / peak, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": dms / dl,
                          "traffic": traffic},
             "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 3)} for k, v in timing.items()},

@@ -8,8 +8,10 @@ Knobs (engine options, include/bk_engine.h):
   split_w2     qubits of the S2 pass (the rest go to S3), 0 = engine default;
   e_source     E(s) for the diagonal phase: 0 = uint16 table, 1 = recomputed
                from popcounts in the pass (no E traffic, more arithmetic);
-  a1_wide      per-pass schedule: the A1 pass with 512 threads x 8 elements
-               (1) or 256 x 16 (0).
+  a1_wide      per-pass schedule, the A1 kernel: 0 = 256 threads x 16 elements
+               (element bits 0-11), 1 = 512 x 8, 2 = warp-local (element bits
+               0-8 inside each warp, no CTA barrier; the strided passes take
+               bits 9 and up; up to 27 element bits).
 For the batched engine the knob is the task-block lag between a statevector
 slab's A1 and S2 tasks.
 
@@ -61,6 +63,12 @@ def candidates(n, precision):
             out.append(dict(engine_mode=1, slab_lag=3, split_w2=w, e_source=0, a1_wide=wide))
         for lag in (1, 2, 3, 4, 6):
             out.append(dict(engine_mode=0, slab_lag=lag, split_w2=w, e_source=0, a1_wide=0))
+    # warp-local A1 (per-pass): np - 9 strided bits, the default split and its neighbours
+    rest9 = np_ - 9
+    if 1 <= rest9 <= 18:
+        d9 = default_w2(rest9)
+        for w in [0] + [w for w in (d9 - 1, d9 + 1) if 3 <= w <= 9 and w <= rest9 and rest9 - w <= 9]:
+            out.append(dict(engine_mode=1, slab_lag=3, split_w2=w, e_source=0, a1_wide=2))
     # E recomputed in the pass, on the default split of both schedules
     out.append(dict(engine_mode=1, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))
     out.append(dict(engine_mode=0, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))

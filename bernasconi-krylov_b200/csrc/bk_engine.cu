@@ -92,7 +92,7 @@ struct bk_ctx {
   int engine_mode = 0;        // 0 persistent dataflow, 1 one launch per pass (tile grid)
   int force_w2 = 0;           // S2 width when > 0 and valid for the size (else the default split)
   int e_recompute = 0;        // tile engine: 1 = E(s) recomputed from popcounts in A1, 0 = uint16 table
-  int a1_wide = 0;            // per-pass schedule: 1 = A1 with 512 threads x 8 elements
+  int a1_wide = 0;            // per-pass schedule A1: 1 = 512 threads x 8 elements, 2 = warp-local (bits 0-8)
   std::map<int, uint16_t*> batch_E;  // E tables of batched runs, per n
   void* d_batch_state = nullptr;
   size_t batch_state_cap = 0;
@@ -283,6 +283,27 @@ int build_amp_map(bk_ctx* c, void* base, int n, int prec, int cp, int h0, int w,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(c, BK_ERR_CUDA, "cuTensorMapEncodeTiled(amp) failed: %d", (int)r);
+  return BK_OK;
+}
+
+// A1 tiles (4096 16-byte elements, element bits [0, 12)) as 128-byte rows with the
+// 128-byte TMA swizzle, for the warp-local A1: dims (16, 256, 2, tiles) of
+// 8-byte units, box (16, 256, 2, 1); the tile index is coordinate 3.
+int build_a1_swizzled_map(bk_ctx* c, void* base, int np, TmaDesc* out) {
+  auto enc = encode_fn();
+  if (!enc) return fail(c, BK_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable from the driver");
+  const uint64_t total = (1ull << np) * 16;
+  cuuint64_t gdim[5] = {16, 256, 2, 1ull << (np - kElemBits), 1};
+  cuuint64_t gstride[4] = {128, 32768, 65536, total};
+  cuuint32_t box[5] = {16, 256, 2, 1, 1};
+  cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  CUresult r = enc(&out->map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, base, gdim, gstride, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(c, BK_ERR_CUDA, "cuTensorMapEncodeTiled(A1, swizzled) failed: %d", (int)r);
+  out->mid_dim = -1;
+  out->hi_dim = 3;
+  out->mid_bits = 0;
   return BK_OK;
 }
 
@@ -576,23 +597,32 @@ int split_w2(const bk_ctx* c, int rest) {
 
 template <class R>
 int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double angle_unit,
-                    const std::vector<R>& tans, const std::vector<R>& scales, PersistRun<R>* run) {
+                    const std::vector<R>& tans, const std::vector<R>& scales, PersistRun<R>* run,
+                    bool grid_mode = false) {
   const int n = p->n;
   const bool c64 = sizeof(R) == 4;
   const int np = c64 ? n - 1 : n;  // element bits
-  const int rest = np - kElemBits;
-  if (rest < 1) return fail(c, BK_ERR_UNSUPPORTED, "persistent engine needs n > %d", kElemBits + (c64 ? 1 : 0));
-  const int w2 = split_w2(c, rest);
+  if (np - kElemBits < 1)
+    return fail(c, BK_ERR_UNSUPPORTED, "persistent engine needs n > %d", kElemBits + (c64 ? 1 : 0));
+  // the warp-local A1 (per-pass schedule) covers element bits 0-8; the strided
+  // passes then take the remaining np - 9 <= 18 bits, the S2 width at least 3
+  // (its tile keeps 12 - w2 <= 9 contiguous bits)
+  const bool a1_warp = grid_mode && c->a1_wide == 2 && np - kA1WarpBits <= 18;
+  const int a1_bits = a1_warp ? kA1WarpBits : kElemBits;
+  const int rest = np - a1_bits;
+  int w2 = split_w2(c, rest);
+  if (a1_warp && w2 < 3) w2 = (rest <= 9) ? rest : (rest + 1) / 2;
   const int w3 = rest - w2;
   if (w2 > 9 || w3 > 9) return fail(c, BK_ERR_UNSUPPORTED, "n = %d needs more than two strided passes", n);
   const int e_tile_bits = c64 ? 13 : 12;
 
   // tensor maps in element space (16-byte elements = two 8-byte TMA elements)
-  TmaDesc a1m, em, m2, m3;
+  TmaDesc a1m, em, m2, m3, a1s;
   BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits, kElemBits, 0, &a1m));
   BK_TRY(build_e_map(c, c->d_E, n, e_tile_bits, &em));
-  BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w2, kElemBits, w2, &m2));
-  if (w3 > 0) BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w3, kElemBits + w2, w3, &m3));
+  BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w2, a1_bits, w2, &m2));
+  if (w3 > 0) BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w3, a1_bits + w2, w3, &m3));
+  if (a1_warp) BK_TRY(build_a1_swizzled_map(c, c->d_state, np, &a1s));
 
   // phase
   typename PhaseV<R>::params ph{};
@@ -610,7 +640,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
 
   // tasks of one step: A1 of slab h+1 is queued ahead of S2 of slab h (L2 hand-off)
   const uint32_t n_a1 = 1u << (np - kElemBits), n_s2 = n_a1, n_s3 = w3 > 0 ? n_a1 : 0u;
-  const uint32_t slabs = 1u << (np - kElemBits - w2);
+  const uint32_t slabs = 1u << std::max(0, np - kElemBits - w2);
   const uint32_t per_slab = 1u << w2;
   std::vector<unsigned long long> tasks;
   tasks.reserve(n_a1 + n_s2 + n_s3);
@@ -621,20 +651,20 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   // ~2 tasks per CTA in flight that the slab is finished, close enough that its
   // data is still in L2 (lag x slab bytes of dirty lines)
   const uint32_t lag = std::max<uint32_t>(1u, std::min<uint32_t>(slabs, (uint32_t)c->slab_lag));
-  for (uint32_t h = 0; h < slabs + lag; ++h) {
+  for (uint32_t h = 0; !a1_warp && h < slabs + lag; ++h) {
     if (h < slabs)
       for (uint32_t j = 0; j < per_slab; ++j) tasks.push_back(task(TASK_A1, 0, h * per_slab + j));
     if (h >= lag)
       for (uint32_t j = 0; j < per_slab; ++j) tasks.push_back(task(TASK_S2, 0, (h - lag) * per_slab + j));
   }
-  for (uint32_t j = 0; j < n_s3; ++j) tasks.push_back(task(TASK_S3, 0, j));
+  for (uint32_t j = 0; !a1_warp && j < n_s3; ++j) tasks.push_back(task(TASK_S3, 0, j));
   std::vector<unsigned long long> final_tasks;
   if (S.slot[(size_t)p->n_steps] >= 0)
     for (uint32_t j = 0; j < n_a1; ++j) final_tasks.push_back(task(TASK_M, 0, j));
 
   // device buffer layout
   Bump b;
-  const size_t o_maps = b.take(4 * sizeof(CUtensorMap));
+  const size_t o_maps = b.take(5 * sizeof(CUtensorMap));
   const size_t o_desc = b.take(sizeof(InstDesc<R>));
   const size_t o_tasks = b.take(tasks.size() * 8);
   const size_t o_final = b.take(std::max<size_t>(final_tasks.size(), 1) * 8);
@@ -657,7 +687,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   int* err = reinterpret_cast<int*>(ctr + slabs + 4);
   int* abort_w = reinterpret_cast<int*>(ctr + slabs + 5);
 
-  CUtensorMap maps[4] = {a1m.map, em.map, m2.map, w3 > 0 ? m3.map : m2.map};
+  CUtensorMap maps[5] = {a1m.map, em.map, m2.map, w3 > 0 ? m3.map : m2.map, a1_warp ? a1s.map : a1m.map};
   InstDesc<R> D{};
   D.state = static_cast<unsigned char*>(c->d_state);
   D.map_a1 = d_maps + 0;
@@ -692,6 +722,8 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   D.n_s2 = n_s2;
   D.n_s3 = n_s3;
   D.e_recompute = c->e_recompute;
+  D.a1_bits = a1_bits;
+  D.map_a1s = d_maps + 4;
 
   cudaStream_t st = c->stream;
   BK_CUDA(c, cudaMemcpyAsync(d_maps, maps, sizeof(maps), cudaMemcpyHostToDevice, st));
@@ -769,7 +801,7 @@ template <class R>
 int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double angle_unit,
                    const std::vector<R>& tans, const std::vector<R>& scales) {
   PersistRun<R> run;
-  BK_TRY(persist_prepare<R>(c, p, S, angle_unit, tans, scales, &run));
+  BK_TRY(persist_prepare<R>(c, p, S, angle_unit, tans, scales, &run, c->engine_mode == 1));
   const int n = p->n;
   cudaStream_t st = c->stream;
   unsigned int* ctr = run.ctr;
@@ -782,6 +814,7 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
     // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_pass_kernel<R>), PersistSmem::kBytes));
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_wide_kernel<R>), PersistSmem::kBytes));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R>), kA1WarpSmem));
     using SampT = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
     BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
     for (int k = 0; k <= p->n_steps; ++k) {
@@ -798,7 +831,9 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
         break;
       }
       BK_TRY(ev_begin(c, "tile_a1", &ev));
-      if (c->a1_wide)
+      if (D.a1_bits == kA1WarpBits)
+        tile_a1_warp_kernel<R><<<n_a1, kComputeThreads, kA1WarpSmem, st>>>(D, (uint32_t)k, err);
+      else if (c->a1_wide == 1)
         tile_a1_wide_kernel<R><<<n_a1, kA1WideThreads, PersistSmem::kBytes, st>>>(D, (uint32_t)k, err);
       else
         tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_A1, (uint32_t)k, err);
@@ -1912,7 +1947,7 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
       c->e_recompute = (int)value;
       return BK_OK;
     case BK_OPT_A1_WIDE:
-      if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "A1 width %lld", (long long)value);
+      if (value < 0 || value > 2) return fail(c, BK_ERR_INVALID, "A1 kernel %lld", (long long)value);
       c->a1_wide = (int)value;
       return BK_OK;
     default:

@@ -274,6 +274,8 @@ struct InstDesc {
   double* results;               // [rows][4]
   uint32_t n_a1, n_s2, n_s3;     // tiles per step
   int e_recompute;               // 1: A1 / M recompute E(s) from popcounts instead of reading the E tile
+  int a1_bits;                   // element bits the A1 pass butterflies (12; 9 for the warp-local A1)
+  const CUtensorMap* map_a1s;    // warp-local A1: the A1 tile with the 128-byte TMA swizzle
 };
 
 struct Program {
@@ -979,12 +981,134 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
     const bool s2 = (kind == TASK_S2);
     const int w = s2 ? D.w2 : D.w3;
     const int mb = s2 ? D.s2_mid_bits : D.s3_mid_bits;
-    const uint32_t h0 = s2 ? (uint32_t)kElemBits : (uint32_t)(kElemBits + D.w2);
+    const uint32_t h0 = s2 ? (uint32_t)D.a1_bits : (uint32_t)(D.a1_bits + D.w2);
     const uint32_t cp = (uint32_t)(kElemBits - w);
     const uint32_t mid = m.tile & ((1u << mb) - 1u), hi = m.tile >> mb;
     const uint32_t tile_base = (mid << cp) | (hi << (h0 + (uint32_t)w));
     process_s_dispatch<R>(w, stage, D.state, tile_base, h0, D.tan[step], none);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-local A1 (per-pass schedule, up to 27 element bits): the pass butterflies
+// element bits 0-8 (+ amplitude bit 0 for complex64), so every warp owns the
+// contiguous 512-element block of the tile with its warp bits 9-11 and both
+// rounds stay inside the warp: no CTA barrier. The tile arrives through the
+// 128-byte TMA swizzle (16-byte chunk address bits 4-6 ^= bits 7-9), which makes
+// round 1 (register bits 0-2, 6; lane bits 3-5, 7, 8) conflict free; round 2
+// (register bits 3-5, 7; lane bits 0-2, 6, 8) reads the engine's XOR swizzle
+// and does bit 8 across lanes 16 apart, then stores 128-byte runs. The strided
+// passes cover element bits 9 and up.
+// ---------------------------------------------------------------------------
+struct PlanA1Warp {
+  static constexpr uint32_t R1_REG = 0x047, R1_LANE = 0x1B8;
+  static constexpr uint32_t R2_REG = 0x0B8, R2_LANE = 0x147;
+  static constexpr uint32_t WARP = 0xE00;
+  static constexpr int kShuffleLanes = 16;  // tile bit 8 = round-2 lane bit 4
+};
+constexpr int kA1WarpBits = 9;
+constexpr int kA1WarpSmem = PersistSmem::kBytes + 1024;  // + room to align the stage to 1024 bytes
+
+// E of 8 consecutive elements starting at `e` (a multiple of 8): complex64 a
+// uint32 pair per element, complex128 a uint16
+template <class R>
+__device__ __forceinline__ void load_e8(const unsigned char* etile, uint32_t e, uint32_t (&ev)[8]) {
+  if constexpr (sizeof(R) == 4) {
+    const uint4 a = *reinterpret_cast<const uint4*>(etile + 4u * e);
+    const uint4 b = *reinterpret_cast<const uint4*>(etile + 4u * e + 16u);
+    ev[0] = a.x; ev[1] = a.y; ev[2] = a.z; ev[3] = a.w;
+    ev[4] = b.x; ev[5] = b.y; ev[6] = b.z; ev[7] = b.w;
+  } else {
+    const uint4 a = *reinterpret_cast<const uint4*>(etile + 2u * e);
+    const uint32_t w[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      ev[2 * q] = w[q] & 0xFFFFu;
+      ev[2 * q + 1] = w[q] >> 16;
+    }
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kComputeThreads, 2)
+    tile_a1_warp_kernel(const __grid_constant__ InstDesc<R> D, uint32_t step, int* err) {
+  using PL = PlanA1Warp;
+  using E = El<R>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar;
+  __shared__ int last_flag;
+  // the swizzled TMA destination must sit on a 1024-byte boundary
+  unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
+  unsigned char* tile = smem;
+  const unsigned char* etile = smem + kStageTileBytes;
+  unsigned char* phase_smem = smem + PersistSmem::kPhaseOff;
+  double* red = reinterpret_cast<double*>(smem + PersistSmem::kRedOff);
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t fb = smem_addr(&full_bar);
+  const uint32_t t_idx = blockIdx.x;
+  const uint32_t tile_base = t_idx << kElemBits;
+  if (tid == 0) {
+    mbar_init(fb, 1);
+    fence_barrier_init();
+    const bool e_tile = !D.e_recompute;
+    mbar_arrive_expect_tx(fb, (uint32_t)kStageTileBytes + (e_tile ? 4096u * 2u * (uint32_t)E::kAmps : 0u));
+    const uint64_t pol = policy_evict_first();
+    tma_load_5d_hint(smem_addr(tile), D.map_a1s, 0, 0, 0, (int)t_idx, 0, fb, pol);
+    if (e_tile) tma_load_5d_hint(smem_addr(tile + kStageTileBytes), D.map_e, 0, 0, (int)t_idx, 0, 0, fb, pol);
+  }
+  PhaseV<R>::stage(D.phase, phase_smem, (int)tid, kComputeThreads);
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(fb, 0, err);
+  if (__syncthreads_or(!ok)) return;
+  typename E::T v[16];
+  const R t = D.tan[step];
+  const int slot = D.slot[step];
+  MeasureAcc acc;
+  // round 1 through the TMA swizzle (tile is 1024-byte aligned, so the swizzle
+  // is a function of the tile offset)
+  const uint32_t b1 = pdep(lane, PL::R1_LANE) | pdep(warp, PL::WARP);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const uint32_t e = b1 | pdep((uint32_t)j, PL::R1_REG);
+    v[j] = E::ld(tile + 16u * (e ^ ((e >> 3) & 7u)));
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t eb = b1 | ((uint32_t)h << 6);
+    uint32_t ev[8];
+    if (D.e_recompute) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) ev[q] = recompute_e<R>(tile_base | eb | (uint32_t)q, D.n);
+    } else {
+      load_e8<R>(etile, eb, ev);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int j = 8 * h + q;
+      if (slot >= 0) measure_el(acc, v[j], ev[q], tile_base | eb | (uint32_t)q, D.e0, D.s0);
+      PhaseV<R>::apply(v[j], ev[q], D.phase, phase_smem, false);
+      E::bfly_inner(v[j], t);
+    }
+  }
+  const R sc = D.scale[step];
+  if (sc != (R)1) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) E::scale(v[j], sc);
+  }
+  el_bflys<R, PL::R1_REG, PL::R1_REG>(v, t);
+  warp_sync();  // round-1 reads vs swizzled stores: same warp
+  el_store_swz<R, PL::R1_REG>(tile, v, b1);
+  warp_sync();  // rounds 1 and 2 share the warp bits
+  const uint32_t b2 = pdep(lane, PL::R2_LANE) | pdep(warp, PL::WARP);
+  el_load<R, PL::R2_REG, true>(tile, v, b2);
+  el_bflys<R, PL::R2_REG, PL::R2_REG>(v, t);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const typename E::T q = E::shfl_xor(v[j], PL::kShuffleLanes);
+    E::bfly_partner(v[j], q, t);
+  }
+  el_gstore<R, PL::R2_REG, kElemBits>(D.state, v, tile_base, b2, 0, policy_evict_last());
+  if (slot >= 0) compute_reduce(acc, D.partials, D.ticket, D.results, slot, t_idx, D.n_a1, red, &last_flag);
 }
 
 }  // namespace bk

@@ -273,8 +273,12 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *   BK_OPT_E_SOURCE: where the diagonal phase and P_< get E(s): 0 = the cached
  *       uint16 table (read with the A1 tile), 1 = recomputed in the pass from the
  *       popcount form C_k = (n-k) - 2 popcount((x ^ (x >> k)) & (2^(n-k) - 1));
- *   BK_OPT_A1_WIDE: per-pass schedule (mode 1), 1 = the A1 pass with 512 threads
- *       of 8 elements (more warps per SM for the diagonal phase), 0 = 256 x 16. */
+ *   BK_OPT_A1_WIDE: per-pass schedule (mode 1), the A1 kernel: 0 = 256 threads x
+ *       16 elements over element bits 0-11, 1 = 512 threads x 8 elements (more
+ *       warps per SM for the diagonal phase), 2 = warp-local: the A1 pass covers
+ *       element bits 0-8, one warp per 512-element block with no CTA barrier,
+ *       and the strided passes take bits 9 and up (sizes up to 27 element bits;
+ *       larger sizes run value 0). */
 enum { BK_OPT_ENGINE_MODE = 0, BK_OPT_SLAB_LAG = 1, BK_OPT_SPLIT_W2 = 2, BK_OPT_E_SOURCE = 3, BK_OPT_A1_WIDE = 4 };
 int bk_set_option(bk_ctx* ctx, int option, int64_t value);
 int bk_get_option(const bk_ctx* ctx, int option, int64_t* value);

@@ -113,3 +113,43 @@ def test_wide_a1_matches_oracle_c128(eng):
     finally:
         eng.set_option("a1_wide", 0)
         eng.set_option("engine_mode", 0)
+
+
+@pytest.mark.gpu
+def test_warp_local_a1_matches_oracle(eng):
+    """The warp-local A1 of the per-pass schedule (BK_OPT_A1_WIDE = 2: element
+    bits 0-8 in one warp per 512-element block, the strided passes from bit 9):
+    complex128 series within 1e-10 of the oracle for a one-strided-pass size
+    (n = 17: S2 = 8 bits) and a two-pass size with the default and forced
+    splits (n = 22: 7 + 6 by default, 4 + 9 and 9 + 4 forced);
+    complex64 within 1e-6 of the 256-thread A1 at n = 24 with the table and the
+    recomputed E, and at n = 28 (S2 = S3 = 9 bits); norms within 1e-5."""
+    eng.set_option("engine_mode", 1)
+    try:
+        eng.set_option("a1_wide", 2)
+        for n, w2 in ((17, 0), (22, 0), (22, 4), (22, 9)):
+            bits, e0 = bk.select_trap(n, 6, 200, 0.05)
+            eng.set_option("split_w2", w2)
+            p, d, nn = eng.evolve(n, bits, 0.35, 0.02, 12, measure=range(0, 13, 3), e0=e0, precision=bk.BK_C128)
+            po, do, no = O.trotter_evolve(n, bits, e0, 0.35, 0.02, 12, measure=list(range(0, 13, 3)))
+            assert np.max(np.abs(p - po)) <= 1e-10, (n, w2)
+            assert np.max(np.abs(d - do)) <= 1e-10 * n, (n, w2)
+            assert np.max(np.abs(nn - no)) <= 1e-10, (n, w2)
+        eng.set_option("split_w2", 0)
+        for n, steps, e_source in ((24, 30, 0), (24, 30, 1), (28, 8, 0)):
+            b2, e2 = bk.select_trap(n, 6, 200, 0.05)
+            eng.set_option("e_source", e_source)
+            out = {}
+            for kernel in (0, 2):
+                eng.set_option("a1_wide", kernel)
+                out[kernel] = eng.evolve(n, b2, 0.35, 0.02, steps, measure=range(0, steps + 1, 2), e0=e2,
+                                         precision=bk.BK_C64)
+            (pw, dw, nw), (ps, ds, ns) = out[2], out[0]
+            assert np.max(np.abs(pw - ps)) <= 1e-6 and np.max(np.abs(dw - ds)) <= 1e-6 * n, (n, e_source)
+            # the complex64 norm itself drifts ~1e-6 over 30 steps (FP32 sums)
+            assert np.max(np.abs(nw - ns)) <= 1e-5, (n, e_source)
+    finally:
+        eng.set_option("a1_wide", 0)
+        eng.set_option("e_source", 0)
+        eng.set_option("split_w2", 0)
+        eng.set_option("engine_mode", 0)
