@@ -483,7 +483,11 @@ def main():
                       "norm_last": float(n_last[-1])}}
 
     if rank == 0 and world == 1 and not a.no_compare:
+        from bk_b200 import tune
         cmp = {}
+        # the complex128 runs use complex128's own tuned knobs (else the engine defaults)
+        if tune.apply(eng, n, bk.BK_C128) is None:
+            tune.apply_config(eng, tune.DEFAULTS)
         for name, pr, meth, steps in (("c128_fused", bk.BK_C128, bk.BK_FUSED, 40),
                                       ("c128_plain", bk.BK_C128, bk.BK_PLAIN, 20)):
             eng.evolve(n, bits, a.g, a.dt, 2, measure=[0], e0=e0, precision=pr, method=meth)
