@@ -57,6 +57,8 @@ struct AdjDesc {
   unsigned int* ticket;
   double* cross;                  // [T] sum over rounds of the weighted Im <lambda|G|psi>
   uint32_t n_a1, n_s2, n_s3;
+  int a1_bits;                    // element bits of the reverse A1 pass (12; 9 for the warp-local A1)
+  const CUtensorMap* map_a1s;     // [2]: warp-local A1 tiles of psi, lambda (128-byte TMA swizzle)
 };
 
 struct AdjSmem {
@@ -66,6 +68,7 @@ struct AdjSmem {
   static constexpr int kPhaseOff = kEOff + kStageEBytes;
   static constexpr int kRedOff = kPhaseOff + 3328;
   static constexpr int kBytes = kRedOff + 256;
+  static constexpr int kAlloc = kBytes + 1024;  // + room to align the stage to 1024 bytes (swizzled TMA)
 };
 
 __host__ __device__ constexpr int popc_c(uint32_t x) { return x ? (int)(x & 1u) + popc_c(x >> 1) : 0; }
@@ -222,6 +225,100 @@ __device__ __forceinline__ double adj_a1(unsigned char* sp, unsigned char* sl, c
   return acc;
 }
 
+// Warp-local reverse A1 (element bits 0-8, one warp per 512-element block of
+// both statevectors; the tile layout of the forward warp-local A1): D^dagger,
+// rescale, amplitude bit 0, round 1 (register bits 0-2, 6) and round 2
+// (register bits 3-5, 7) with their cross terms, bit 8 across lanes 16 apart.
+// The only CTA barrier releases the stage after round 2's reads.
+template <class R, class F>
+__device__ __forceinline__ double adj_a1_warp(unsigned char* sp, unsigned char* sl, const unsigned char* etile,
+                                              const AdjDesc<R>& D, uint32_t t_idx, uint32_t j, bool phase_on,
+                                              const unsigned char* phase_smem, F&& stage_free) {
+  using PL = PlanA1Warp;
+  using E = El<R>;
+  constexpr bool kC64 = sizeof(R) == 4;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t tile_base = t_idx << kElemBits;
+  const R t = D.tan[j];
+  const R sc = D.scale[j];
+  const double L = D.lg1t2[j];
+  typename E::T v[16], u[16];
+  CrossAcc<R> ca;
+  double acc = 0.0;
+  const uint32_t b1 = pdep(lane, PL::R1_LANE) | pdep(warp, PL::WARP);
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const uint32_t e = b1 | pdep((uint32_t)q, PL::R1_REG);
+    const uint32_t o = 16u * (e ^ ((e >> 3) & 7u));  // 128-byte TMA swizzle (stage 1024-byte aligned)
+    v[q] = E::ld(sp + o);
+    u[q] = E::ld(sl + o);
+  }
+  if (phase_on) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint32_t ev[8];
+      load_e8<R>(etile, b1 | ((uint32_t)h << 6), ev);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        // one set of rotation coefficients for both statevectors
+        const typename PhaseV<R>::Coef cf = PhaseV<R>::coef(ev[q], D.phase, phase_smem, true);
+        PhaseV<R>::rotate(v[8 * h + q], cf, true);
+        PhaseV<R>::rotate(u[8 * h + q], cf, true);
+      }
+    }
+  }
+  if (sc != (R)1) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      E::scale(v[q], sc);
+      E::scale(u[q], sc);
+    }
+  }
+  int m = 0;
+  if constexpr (kC64) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      ca.inner(v[q], u[q]);
+      E::bfly_inner(v[q], t);
+      E::bfly_inner(u[q], t);
+    }
+    acc += ca.take();  // m = 0
+    m = 1;
+  }
+  el_cross<R, PL::R1_REG, PL::R1_REG>(v, u, ca);
+  acc += round_weight(m, L) * ca.take();
+  m += popc_c(PL::R1_REG);
+  el_bflys<R, PL::R1_REG, PL::R1_REG>(v, t);
+  el_bflys<R, PL::R1_REG, PL::R1_REG>(u, t);
+  warp_sync();  // round-1 reads vs swizzled stores: same warp
+  el_store_swz<R, PL::R1_REG>(sp, v, b1);
+  el_store_swz<R, PL::R1_REG>(sl, u, b1);
+  warp_sync();  // rounds 1 and 2 share the warp bits
+  const uint32_t b2 = pdep(lane, PL::R2_LANE) | pdep(warp, PL::WARP);
+  el_load<R, PL::R2_REG, true>(sp, v, b2);
+  el_load<R, PL::R2_REG, true>(sl, u, b2);
+  __syncthreads();
+  stage_free();
+  el_cross<R, PL::R2_REG, PL::R2_REG>(v, u, ca);
+  acc += round_weight(m, L) * ca.take();
+  m += popc_c(PL::R2_REG);
+  el_bflys<R, PL::R2_REG, PL::R2_REG>(v, t);
+  el_bflys<R, PL::R2_REG, PL::R2_REG>(u, t);
+  // tile bit 8 across lanes: each thread adds its own ordered term
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const typename E::T pv = E::shfl_xor(v[q], PL::kShuffleLanes);
+    const typename E::T pu = E::shfl_xor(u[q], PL::kShuffleLanes);
+    ca.one(pv, u[q]);
+    E::bfly_partner(v[q], pv, t);
+    E::bfly_partner(u[q], pu, t);
+  }
+  acc += round_weight(m, L) * ca.take();
+  el_gstore_plain<R, PL::R2_REG, kElemBits>(D.psi, v, tile_base, b2, 0);
+  el_gstore_plain<R, PL::R2_REG, kElemBits>(D.lam, u, tile_base, b2, 0);
+  return acc;
+}
+
 // reverse strided pass of width W (element bits [0, 12 - W) u [h0, h0 + W));
 // m0 = qubits already rotated in this step by the earlier passes
 template <class R, int W, class F>
@@ -308,10 +405,15 @@ __device__ __forceinline__ void adj_issue(const AdjDesc<R>& D, int kind, uint32_
                                           uint32_t fb) {
   if (kind == TASK_A1) {
     mbar_arrive_expect_tx(fb, (uint32_t)(2 * kStageTileBytes + 4096 * 2 * El<R>::kAmps));
-    const int hd = D.a1_hi_dim;
-    const int c2 = hd == 2 ? (int)tile : 0, c3 = hd == 3 ? (int)tile : 0;
-    tma_load_5d(smem_addr(stage + AdjSmem::kPsiOff), D.map_a1 + 0, 0, 0, c2, c3, 0, fb);
-    tma_load_5d(smem_addr(stage + AdjSmem::kLamOff), D.map_a1 + 1, 0, 0, c2, c3, 0, fb);
+    if (D.a1_bits == kA1WarpBits) {
+      tma_load_5d(smem_addr(stage + AdjSmem::kPsiOff), D.map_a1s + 0, 0, 0, 0, (int)tile, 0, fb);
+      tma_load_5d(smem_addr(stage + AdjSmem::kLamOff), D.map_a1s + 1, 0, 0, 0, (int)tile, 0, fb);
+    } else {
+      const int hd = D.a1_hi_dim;
+      const int c2 = hd == 2 ? (int)tile : 0, c3 = hd == 3 ? (int)tile : 0;
+      tma_load_5d(smem_addr(stage + AdjSmem::kPsiOff), D.map_a1 + 0, 0, 0, c2, c3, 0, fb);
+      tma_load_5d(smem_addr(stage + AdjSmem::kLamOff), D.map_a1 + 1, 0, 0, c2, c3, 0, fb);
+    }
     tma_load_5d(smem_addr(stage + AdjSmem::kEOff), D.map_e, 0, 0, (int)tile, 0, 0, fb);
   } else {
     const bool s2 = (kind == TASK_S2);
@@ -336,9 +438,11 @@ template <class R>
 __global__ void __launch_bounds__(kComputeThreads, 1)
     adj_pass_kernel(const __grid_constant__ AdjDesc<R> D, int kind, uint32_t j, int phase_on, int last_pass,
                     int* err) {
-  extern __shared__ __align__(1024) unsigned char smem[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar;
   __shared__ int is_last;
+  // the stage sits on a 1024-byte boundary (the warp-local A1's swizzled TMA needs it)
+  unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
   unsigned char* stage = smem;
   unsigned char* phase_smem = smem + AdjSmem::kPhaseOff;
   double* red = reinterpret_cast<double*>(smem + AdjSmem::kRedOff);
@@ -347,10 +451,10 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
   const uint32_t ntiles = kind == TASK_A1 ? D.n_a1 : (kind == TASK_S2 ? D.n_s2 : D.n_s3);
   const uint32_t part0 = kind == TASK_A1 ? 0u : (kind == TASK_S2 ? D.n_a1 : D.n_a1 + D.n_s2);
   const int w = kind == TASK_S2 ? D.w2 : D.w3;
-  const uint32_t h0 = kind == TASK_S2 ? (uint32_t)kElemBits : (uint32_t)(kElemBits + D.w2);
+  const uint32_t h0 = kind == TASK_S2 ? (uint32_t)D.a1_bits : (uint32_t)(D.a1_bits + D.w2);
   const int mb = kind == TASK_S2 ? D.s2_mid_bits : D.s3_mid_bits;
   // qubits rotated by the earlier passes of the step (complex64: + amplitude bit 0)
-  const int m0 = (sizeof(R) == 4 ? 1 : 0) + kElemBits + (kind == TASK_S3 ? D.w2 : 0);
+  const int m0 = (sizeof(R) == 4 ? 1 : 0) + D.a1_bits + (kind == TASK_S3 ? D.w2 : 0);
   uint32_t tile = blockIdx.x;
   // the first tile's loads go out before the phase tables are staged
   if (tid == 0) {
@@ -370,7 +474,10 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
       if (tid == 0 && nxt < ntiles) adj_issue(D, kind, nxt, stage, fb);
     };
     double acc;
-    if (kind == TASK_A1) {
+    if (kind == TASK_A1 && D.a1_bits == kA1WarpBits) {
+      acc = adj_a1_warp<R>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
+                           phase_on != 0, phase_smem, stage_free);
+    } else if (kind == TASK_A1) {
       acc = adj_a1<R>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
                       phase_on != 0, phase_smem, stage_free);
     } else {

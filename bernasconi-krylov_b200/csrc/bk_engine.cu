@@ -93,6 +93,7 @@ struct bk_ctx {
   int force_w2 = 0;           // S2 width when > 0 and valid for the size (else the default split)
   int e_recompute = 0;        // tile engine: 1 = E(s) recomputed from popcounts in A1, 0 = uint16 table
   int a1_wide = 0;            // per-pass schedule A1: 1 = 512 threads x 8 elements, 2 = warp-local (bits 0-8)
+  int adj_a1 = 2;             // adjoint reverse sweep A1: 0 = 12-bit, 1 = warp-local (bits 0-8), 2 = automatic
   std::map<int, uint16_t*> batch_E;  // E tables of batched runs, per n
   void* d_batch_state = nullptr;
   size_t batch_state_cap = 0;
@@ -1480,7 +1481,17 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   // reverse-sweep bookkeeping on the host: tangents, rescales, round-weight
   // logs, the log2 scale of both vectors at each step's cross terms, resets
   const InstDesc<R>& FD = run.D;
-  const int w2 = FD.w2, w3 = FD.w3;
+  // reverse pass geometry: the warp-local A1 (element bits 0-8) when chosen and
+  // the strided passes can take the remaining np - 9 <= 18 bits, else the
+  // forward's 12-bit A1 split
+  // (automatic: only where the 12-bit geometry needs three passes anyway, so
+  // the warp-local A1 adds none)
+  const bool warp_fits = np - kA1WarpBits <= 18;
+  const bool adj_warp = warp_fits && (c->adj_a1 == 1 || (c->adj_a1 == 2 && np - kElemBits > 9));
+  const int a1r = adj_warp ? kA1WarpBits : kElemBits;
+  const int rest_r = np - a1r;
+  const int w2 = adj_warp ? ((rest_r <= 9) ? rest_r : (rest_r + 1) / 2) : FD.w2;
+  const int w3 = adj_warp ? rest_r - w2 : FD.w3;
   std::vector<R> t_rev((size_t)T), sc_rev((size_t)T);
   std::vector<double> lg_rev((size_t)T);
   std::vector<long double> wlog2((size_t)T);
@@ -1514,9 +1525,9 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   }
 
   // device layout
-  const uint32_t n_a1 = FD.n_a1, n_s2 = FD.n_s2, n_s3 = FD.n_s3;
+  const uint32_t n_a1 = FD.n_a1, n_s2 = FD.n_s2, n_s3 = w3 > 0 ? n_a1 : 0u;
   Bump b;
-  const size_t o_maps = b.take(7 * sizeof(CUtensorMap));
+  const size_t o_maps = b.take(9 * sizeof(CUtensorMap));
   const size_t o_tan = b.take((size_t)T * sizeof(R));
   const size_t o_sc = b.take((size_t)T * sizeof(R));
   const size_t o_lg = b.take((size_t)T * sizeof(double));
@@ -1532,20 +1543,27 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   double* d_cross = reinterpret_cast<double*>(base + o_cross);
   double* d_dev = reinterpret_cast<double*>(base + o_dev);
 
-  TmaDesc a1p, a1l, em, s2p, s2l, s3p, s3l;
+  TmaDesc a1p, a1l, em, s2p, s2l, s3p, s3l, a1sp, a1sl;
   BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits, kElemBits, 0, &a1p));
   BK_TRY(build_amp_map(c, c->d_lam, np, BK_C128, kElemBits, kElemBits, 0, &a1l));
   BK_TRY(build_e_map(c, c->d_E, n, kC64 ? 13 : 12, &em));
-  BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w2, kElemBits, w2, &s2p));
-  BK_TRY(build_amp_map(c, c->d_lam, np, BK_C128, kElemBits - w2, kElemBits, w2, &s2l));
+  BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w2, a1r, w2, &s2p));
+  BK_TRY(build_amp_map(c, c->d_lam, np, BK_C128, kElemBits - w2, a1r, w2, &s2l));
   if (w3 > 0) {
-    BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w3, kElemBits + w2, w3, &s3p));
-    BK_TRY(build_amp_map(c, c->d_lam, np, BK_C128, kElemBits - w3, kElemBits + w2, w3, &s3l));
+    BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w3, a1r + w2, w3, &s3p));
+    BK_TRY(build_amp_map(c, c->d_lam, np, BK_C128, kElemBits - w3, a1r + w2, w3, &s3l));
   } else {
     s3p = s2p;
     s3l = s2l;
   }
-  CUtensorMap maps[7] = {a1p.map, a1l.map, em.map, s2p.map, s2l.map, s3p.map, s3l.map};
+  if (adj_warp) {
+    BK_TRY(build_a1_swizzled_map(c, c->d_state, np, &a1sp));
+    BK_TRY(build_a1_swizzled_map(c, c->d_lam, np, &a1sl));
+  } else {
+    a1sp = a1p;
+    a1sl = a1l;
+  }
+  CUtensorMap maps[9] = {a1p.map, a1l.map, em.map, s2p.map, s2l.map, s3p.map, s3l.map, a1sp.map, a1sl.map};
   AdjDesc<R> A{};
   A.psi = static_cast<unsigned char*>(c->d_state);
   A.lam = static_cast<unsigned char*>(c->d_lam);
@@ -1574,12 +1592,14 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   A.n_a1 = n_a1;
   A.n_s2 = n_s2;
   A.n_s3 = n_s3;
+  A.a1_bits = a1r;
+  A.map_a1s = d_maps + 7;
   BK_CUDA(c, cudaMemcpyAsync(d_maps, maps, sizeof(maps), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_tan, t_rev.data(), (size_t)T * sizeof(R), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_sc, sc_rev.data(), (size_t)T * sizeof(R), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_lg, lg_rev.data(), (size_t)T * sizeof(double), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemsetAsync(base + o_ctr, 0, 64, st));
-  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(adj_pass_kernel<R>), AdjSmem::kBytes));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(adj_pass_kernel<R>), AdjSmem::kAlloc));
   const int ns = c->num_sms;
   const unsigned g1 = std::min<unsigned>(n_a1, (unsigned)ns), g2 = std::min<unsigned>(n_s2, (unsigned)ns),
                  g3 = std::min<unsigned>(std::max<unsigned>(n_s3, 1u), (unsigned)ns);
@@ -1598,16 +1618,16 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   for (int j = 0; j < T; ++j) {
     size_t e = 0;
     BK_TRY(ev_begin(c, "adj_a1", &e));
-    adj_pass_kernel<R><<<g1, kComputeThreads, AdjSmem::kBytes, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0, err);
+    adj_pass_kernel<R><<<g1, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0, err);
     BK_CUDA(c, cudaGetLastError());
     BK_TRY(ev_end(c, e));
     BK_TRY(ev_begin(c, "adj_s2", &e));
-    adj_pass_kernel<R><<<g2, kComputeThreads, AdjSmem::kBytes, st>>>(A, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1, err);
+    adj_pass_kernel<R><<<g2, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1, err);
     BK_CUDA(c, cudaGetLastError());
     BK_TRY(ev_end(c, e));
     if (w3 > 0) {
       BK_TRY(ev_begin(c, "adj_s3", &e));
-      adj_pass_kernel<R><<<g3, kComputeThreads, AdjSmem::kBytes, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
+      adj_pass_kernel<R><<<g3, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
       BK_CUDA(c, cudaGetLastError());
       BK_TRY(ev_end(c, e));
     }
@@ -1950,6 +1970,10 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
       if (value < 0 || value > 2) return fail(c, BK_ERR_INVALID, "A1 kernel %lld", (long long)value);
       c->a1_wide = (int)value;
       return BK_OK;
+    case BK_OPT_ADJ_A1:
+      if (value < 0 || value > 2) return fail(c, BK_ERR_INVALID, "adjoint A1 %lld", (long long)value);
+      c->adj_a1 = (int)value;
+      return BK_OK;
     default:
       return fail(c, BK_ERR_INVALID, "unknown option %d", option);
   }
@@ -1963,6 +1987,7 @@ int bk_get_option(const bk_ctx* c, int option, int64_t* value) {
     case BK_OPT_SPLIT_W2: *value = c->force_w2; return BK_OK;
     case BK_OPT_E_SOURCE: *value = c->e_recompute; return BK_OK;
     case BK_OPT_A1_WIDE: *value = c->a1_wide; return BK_OK;
+    case BK_OPT_ADJ_A1: *value = c->adj_a1; return BK_OK;
     default: return BK_ERR_INVALID;
   }
 }

@@ -278,8 +278,20 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       warps per SM for the diagonal phase), 2 = warp-local: the A1 pass covers
  *       element bits 0-8, one warp per 512-element block with no CTA barrier,
  *       and the strided passes take bits 9 and up (sizes up to 27 element bits;
- *       larger sizes run value 0). */
-enum { BK_OPT_ENGINE_MODE = 0, BK_OPT_SLAB_LAG = 1, BK_OPT_SPLIT_W2 = 2, BK_OPT_E_SOURCE = 3, BK_OPT_A1_WIDE = 4 };
+ *       larger sizes run value 0);
+ *   BK_OPT_ADJ_A1: bk_adjoint's reverse sweep, 1 = the warp-local A1 layout for
+ *       both statevectors (element bits 0-8, strided passes from bit 9; up to 27
+ *       element bits), 0 = the 12-bit A1 of the forward geometry, 2 (default) =
+ *       warp-local only where the 12-bit geometry needs two strided passes
+ *       anyway (more than 21 element bits), so it adds no pass. */
+enum {
+  BK_OPT_ENGINE_MODE = 0,
+  BK_OPT_SLAB_LAG = 1,
+  BK_OPT_SPLIT_W2 = 2,
+  BK_OPT_E_SOURCE = 3,
+  BK_OPT_A1_WIDE = 4,
+  BK_OPT_ADJ_A1 = 5
+};
 int bk_set_option(bk_ctx* ctx, int option, int64_t value);
 int bk_get_option(const bk_ctx* ctx, int option, int64_t* value);
 

@@ -137,3 +137,40 @@ def test_adjoint_n28_complex64_against_complex128(eng):
     assert st64["n_checkpoints"] == 3 and st128["max_drift"] <= 1e-11 and st64["max_drift"] <= 1e-4
     assert abs(v64 - v128) <= 1e-6
     assert np.max(np.abs(g64 - g128)) <= 1e-3 * np.max(np.abs(g128))
+
+
+# warp-local reverse A1 (BK_OPT_ADJ_A1 = 1): element bits 0-8 per warp, strided
+# passes from bit 9 — one S2 of 4 bits (n = 13), of 9 bits with the lane-shuffle
+# bit (n = 18), S2 + S3 (n = 22: 7 + 6)
+@pytest.mark.parametrize("n,T,K", [(13, 48, 16), (18, 40, 16), (22, 24, 8)])
+def test_adjoint_warp_local_a1_c128_matches_oracle(eng, n, T, K):
+    bits, e0, gs, seg = _case(n, 6 if T % 6 == 0 else 4, T, n)
+    prev = eng.get_option("adj_a1")
+    eng.set_option("adj_a1", 1)
+    try:
+        val, grad, st = eng.adjoint(n, bits, gs, 0.05, T, e0=e0, precision=bk.BK_C128, checkpoint_every=K,
+                                    per_step=True)
+    finally:
+        eng.set_option("adj_a1", prev)
+    oval, ograd = O.trotter_adjoint(n, bits, e0, gs[seg], 0.05, T)
+    scale = np.max(np.abs(ograd))
+    assert abs(val - oval) <= 1e-10
+    assert np.max(np.abs(st["grad_steps"] - ograd)) <= 1e-9 * scale
+    assert st["max_drift"] <= 1e-11
+
+
+@pytest.mark.parametrize("n", [14, 23])
+def test_adjoint_warp_local_a1_c64_matches_oracle(eng, n):
+    T, K = (24, 8) if n >= 22 else (40, 16)
+    bits, e0, gs, seg = _case(n, 4, T, n)
+    prev = eng.get_option("adj_a1")
+    eng.set_option("adj_a1", 1)
+    try:
+        val, grad, st = eng.adjoint(n, bits, gs, 0.05, T, e0=e0, precision=bk.BK_C64, checkpoint_every=K,
+                                    per_step=True)
+    finally:
+        eng.set_option("adj_a1", prev)
+    oval, ograd = O.trotter_adjoint(n, bits, e0, gs[seg], 0.05, T)
+    assert abs(val - oval) <= 1e-6
+    assert np.max(np.abs(st["grad_steps"] - ograd)) <= 1e-4 * np.max(np.abs(ograd))
+    assert st["max_drift"] <= 1e-4
