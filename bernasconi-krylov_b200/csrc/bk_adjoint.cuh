@@ -57,7 +57,6 @@ struct AdjDesc {
   unsigned int* ticket;
   double* cross;                  // [T] sum over rounds of the weighted Im <lambda|G|psi>
   uint32_t n_a1, n_s2, n_s3;
-  int a1_bits;                    // element bits of the reverse A1 pass (12; 9 for the warp-local A1)
   const CUtensorMap* map_a1s;     // [2]: warp-local A1 tiles of psi, lambda (128-byte TMA swizzle)
 };
 
@@ -400,12 +399,12 @@ __device__ __forceinline__ double adj_s_dispatch(int w, unsigned char* sp, unsig
   }
 }
 
-template <class R>
+template <class R, bool kWarpA1>
 __device__ __forceinline__ void adj_issue(const AdjDesc<R>& D, int kind, uint32_t tile, unsigned char* stage,
                                           uint32_t fb) {
   if (kind == TASK_A1) {
     mbar_arrive_expect_tx(fb, (uint32_t)(2 * kStageTileBytes + 4096 * 2 * El<R>::kAmps));
-    if (D.a1_bits == kA1WarpBits) {
+    if (kWarpA1) {
       tma_load_5d(smem_addr(stage + AdjSmem::kPsiOff), D.map_a1s + 0, 0, 0, 0, (int)tile, 0, fb);
       tma_load_5d(smem_addr(stage + AdjSmem::kLamOff), D.map_a1s + 1, 0, 0, 0, (int)tile, 0, fb);
     } else {
@@ -434,15 +433,18 @@ __device__ __forceinline__ void adj_issue(const AdjDesc<R>& D, int kind, uint32_
 // One reverse pass (kind = TASK_A1 / TASK_S2 / TASK_S3) of reverse step j.
 // Grid: at most one CTA per SM, each loops over tiles blockIdx.x + i gridDim.x.
 // last_pass: the step's last pass also reduces the step's per-tile sums.
-template <class R>
+// kWarpA1: every pass of a warp-local run (A1 in the warp-local layout, strided
+// passes from element bit 9); its own instantiation, so the 12-bit kernel keeps
+// its register allocation.
+template <class R, bool kWarpA1>
 __global__ void __launch_bounds__(kComputeThreads, 1)
     adj_pass_kernel(const __grid_constant__ AdjDesc<R> D, int kind, uint32_t j, int phase_on, int last_pass,
                     int* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar;
   __shared__ int is_last;
-  // the stage sits on a 1024-byte boundary (the warp-local A1's swizzled TMA needs it)
-  unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
+  // warp-local runs: the stage sits on a 1024-byte boundary (swizzled TMA)
+  unsigned char* smem = kWarpA1 ? smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u) : smem_raw;
   unsigned char* stage = smem;
   unsigned char* phase_smem = smem + AdjSmem::kPhaseOff;
   double* red = reinterpret_cast<double*>(smem + AdjSmem::kRedOff);
@@ -451,16 +453,17 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
   const uint32_t ntiles = kind == TASK_A1 ? D.n_a1 : (kind == TASK_S2 ? D.n_s2 : D.n_s3);
   const uint32_t part0 = kind == TASK_A1 ? 0u : (kind == TASK_S2 ? D.n_a1 : D.n_a1 + D.n_s2);
   const int w = kind == TASK_S2 ? D.w2 : D.w3;
-  const uint32_t h0 = kind == TASK_S2 ? (uint32_t)D.a1_bits : (uint32_t)(D.a1_bits + D.w2);
+  constexpr int kA1Bits = kWarpA1 ? kA1WarpBits : kElemBits;  // element bits of the step's A1 pass
+  const uint32_t h0 = kind == TASK_S2 ? (uint32_t)kA1Bits : (uint32_t)(kA1Bits + D.w2);
   const int mb = kind == TASK_S2 ? D.s2_mid_bits : D.s3_mid_bits;
   // qubits rotated by the earlier passes of the step (complex64: + amplitude bit 0)
-  const int m0 = (sizeof(R) == 4 ? 1 : 0) + D.a1_bits + (kind == TASK_S3 ? D.w2 : 0);
+  const int m0 = (sizeof(R) == 4 ? 1 : 0) + kA1Bits + (kind == TASK_S3 ? D.w2 : 0);
   uint32_t tile = blockIdx.x;
   // the first tile's loads go out before the phase tables are staged
   if (tid == 0) {
     mbar_init(fb, 1);
     fence_barrier_init();
-    if (tile < ntiles) adj_issue(D, kind, tile, stage, fb);
+    if (tile < ntiles) adj_issue<R, kWarpA1>(D, kind, tile, stage, fb);
   }
   if (kind == TASK_A1 && phase_on) PhaseV<R>::stage(D.phase, phase_smem, tid, kComputeThreads);
   __syncthreads();
@@ -471,13 +474,13 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
     parity ^= 1u;
     const uint32_t nxt = tile + gridDim.x;
     auto stage_free = [&]() {
-      if (tid == 0 && nxt < ntiles) adj_issue(D, kind, nxt, stage, fb);
+      if (tid == 0 && nxt < ntiles) adj_issue<R, kWarpA1>(D, kind, nxt, stage, fb);
     };
     double acc;
-    if (kind == TASK_A1 && D.a1_bits == kA1WarpBits) {
+    if (kWarpA1 && kind == TASK_A1) {
       acc = adj_a1_warp<R>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
                            phase_on != 0, phase_smem, stage_free);
-    } else if (kind == TASK_A1) {
+    } else if (!kWarpA1 && kind == TASK_A1) {
       acc = adj_a1<R>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
                       phase_on != 0, phase_smem, stage_free);
     } else {

@@ -1592,14 +1592,14 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   A.n_a1 = n_a1;
   A.n_s2 = n_s2;
   A.n_s3 = n_s3;
-  A.a1_bits = a1r;
   A.map_a1s = d_maps + 7;
   BK_CUDA(c, cudaMemcpyAsync(d_maps, maps, sizeof(maps), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_tan, t_rev.data(), (size_t)T * sizeof(R), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_sc, sc_rev.data(), (size_t)T * sizeof(R), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_lg, lg_rev.data(), (size_t)T * sizeof(double), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemsetAsync(base + o_ctr, 0, 64, st));
-  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(adj_pass_kernel<R>), AdjSmem::kAlloc));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(adj_pass_kernel<R, false>), AdjSmem::kAlloc));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(adj_pass_kernel<R, true>), AdjSmem::kAlloc));
   const int ns = c->num_sms;
   const unsigned g1 = std::min<unsigned>(n_a1, (unsigned)ns), g2 = std::min<unsigned>(n_s2, (unsigned)ns),
                  g3 = std::min<unsigned>(std::max<unsigned>(n_s3, 1u), (unsigned)ns);
@@ -1618,16 +1618,29 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   for (int j = 0; j < T; ++j) {
     size_t e = 0;
     BK_TRY(ev_begin(c, "adj_a1", &e));
-    adj_pass_kernel<R><<<g1, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0, err);
+    if (adj_warp)
+      adj_pass_kernel<R, true><<<g1, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0,
+                                                                            err);
+    else
+      adj_pass_kernel<R, false><<<g1, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0,
+                                                                             err);
     BK_CUDA(c, cudaGetLastError());
     BK_TRY(ev_end(c, e));
     BK_TRY(ev_begin(c, "adj_s2", &e));
-    adj_pass_kernel<R><<<g2, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1, err);
+    if (adj_warp)
+      adj_pass_kernel<R, true><<<g2, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1,
+                                                                            err);
+    else
+      adj_pass_kernel<R, false><<<g2, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S2, (uint32_t)j, 0,
+                                                                             w3 > 0 ? 0 : 1, err);
     BK_CUDA(c, cudaGetLastError());
     BK_TRY(ev_end(c, e));
     if (w3 > 0) {
       BK_TRY(ev_begin(c, "adj_s3", &e));
-      adj_pass_kernel<R><<<g3, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
+      if (adj_warp)
+        adj_pass_kernel<R, true><<<g3, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
+      else
+        adj_pass_kernel<R, false><<<g3, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
       BK_CUDA(c, cudaGetLastError());
       BK_TRY(ev_end(c, e));
     }
