@@ -93,7 +93,7 @@ struct bk_ctx {
   int force_w2 = 0;           // S2 width when > 0 and valid for the size (else the default split)
   int e_recompute = 0;        // tile engine: 1 = E(s) recomputed from popcounts in A1, 0 = uint16 table
   int a1_wide = 0;            // per-pass schedule A1: 1 = 512 threads x 8 elements, 2 = warp-local (bits 0-8)
-  int adj_a1 = 2;             // adjoint reverse sweep A1: 0 = 12-bit, 1 = warp-local (bits 0-8), 2 = automatic
+  int adj_a1 = 0;             // adjoint reverse sweep A1: 0 = 12-bit, 1 = warp-local (element bits 0-8)
   std::map<int, uint16_t*> batch_E;  // E tables of batched runs, per n
   void* d_batch_state = nullptr;
   size_t batch_state_cap = 0;
@@ -1484,10 +1484,7 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   // reverse pass geometry: the warp-local A1 (element bits 0-8) when chosen and
   // the strided passes can take the remaining np - 9 <= 18 bits, else the
   // forward's 12-bit A1 split
-  // (automatic: only where the 12-bit geometry needs three passes anyway, so
-  // the warp-local A1 adds none)
-  const bool warp_fits = np - kA1WarpBits <= 18;
-  const bool adj_warp = warp_fits && (c->adj_a1 == 1 || (c->adj_a1 == 2 && np - kElemBits > 9));
+  const bool adj_warp = c->adj_a1 == 1 && np - kA1WarpBits <= 18;
   const int a1r = adj_warp ? kA1WarpBits : kElemBits;
   const int rest_r = np - a1r;
   const int w2 = adj_warp ? ((rest_r <= 9) ? rest_r : (rest_r + 1) / 2) : FD.w2;
@@ -1984,7 +1981,7 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
       c->a1_wide = (int)value;
       return BK_OK;
     case BK_OPT_ADJ_A1:
-      if (value < 0 || value > 2) return fail(c, BK_ERR_INVALID, "adjoint A1 %lld", (long long)value);
+      if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "adjoint A1 %lld", (long long)value);
       c->adj_a1 = (int)value;
       return BK_OK;
     default:

@@ -281,9 +281,7 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       larger sizes run value 0);
  *   BK_OPT_ADJ_A1: bk_adjoint's reverse sweep, 1 = the warp-local A1 layout for
  *       both statevectors (element bits 0-8, strided passes from bit 9; up to 27
- *       element bits), 0 = the 12-bit A1 of the forward geometry, 2 (default) =
- *       warp-local only where the 12-bit geometry needs two strided passes
- *       anyway (more than 21 element bits), so it adds no pass. */
+ *       element bits), 0 (default) = the 12-bit A1 of the forward geometry. */
 enum {
   BK_OPT_ENGINE_MODE = 0,
   BK_OPT_SLAB_LAG = 1,
