@@ -153,3 +153,23 @@ def test_warp_local_a1_matches_oracle(eng):
         eng.set_option("e_source", 0)
         eng.set_option("split_w2", 0)
         eng.set_option("engine_mode", 0)
+
+
+@pytest.mark.gpu
+def test_warp_local_a1_falls_back_above_27_element_bits(eng):
+    """BK_OPT_A1_WIDE = 2 on a size whose strided passes could not take the
+    remaining bits (complex64 n = 30, complex128 n = 28: more than 27 element
+    bits) runs the 256-thread A1 geometry: series bit-identical to value 0."""
+    eng.set_option("engine_mode", 1)
+    try:
+        for n, prec in ((30, bk.BK_C64), (28, bk.BK_C128)):
+            bits, e0 = bk.select_trap(n, 6, 100, 0.05)
+            out = {}
+            for kernel in (0, 2):
+                eng.set_option("a1_wide", kernel)
+                out[kernel] = eng.evolve(n, bits, 0.35, 0.02, 3, measure=[0, 3], e0=e0, precision=prec)
+            for a, b in zip(out[0], out[2]):
+                assert np.array_equal(a, b), n
+    finally:
+        eng.set_option("a1_wide", 0)
+        eng.set_option("engine_mode", 0)
