@@ -14,6 +14,11 @@ reference itself ships:
                               data_processed/probability_dynamics_n{N}.csv (cuStateVec
                               complex128 on H200, dt = 0.05, 1200 steps, every step);
                               N <= 20 keep every point, N >= 24 every 10th point.
+* ``time_series_rows_n{N}.csv`` the header and selected rows, verbatim, of
+                              data_processed/probability_dynamics_n{N}.csv (the connector's
+                              export_time_series_csv output): the file's first row, rows across a
+                              record boundary and rows with P_< > 0 — the byte-level pin of
+                              bk_b200.export's time-series writer.
 """
 import argparse
 import csv
@@ -98,6 +103,15 @@ def main():
                         "dh": s["dh"][::step]})
         json.dump({"source": f"data_processed/probability_dynamics_n{n}.csv", "series": out},
                   open(os.path.join(a.out, f"series_n{n}.json"), "w"), separators=(",", ":"))
+    for n in (16, 28):
+        with open(os.path.join(dp, f"probability_dynamics_n{n}.csv"), newline="") as f:
+            lines = f.read().split("\n")
+        header, rows = lines[0], [x for x in lines[1:] if x]
+        keep = list(range(12)) + list(range(1197, 1206))
+        keep += [i for i, x in enumerate(rows) if float(x.split(",")[5]) > 0.0][:20] + [len(rows) - 2, len(rows) - 1]
+        picked = [rows[i] for i in sorted(set(keep))]
+        with open(os.path.join(a.out, f"time_series_rows_n{n}.csv"), "w", newline="") as f:
+            f.write("\n".join([header] + picked) + "\n")
     print("golden fixtures written to", a.out)
 
 
