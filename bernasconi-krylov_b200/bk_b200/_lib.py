@@ -61,6 +61,16 @@ class AdjointStatsC(ctypes.Structure):
                 ("reverse_ms", ctypes.c_double)]
 
 
+class LanczosParamsC(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("g", ctypes.c_double), ("num_eigenpairs", ctypes.c_int32),
+                ("max_krylov_dim", ctypes.c_int32), ("tolerance", ctypes.c_double), ("normalize_by_n", ctypes.c_int32),
+                ("alphas", ctypes.POINTER(ctypes.c_double)), ("betas", ctypes.POINTER(ctypes.c_double))]
+
+
+class LanczosStatsC(ctypes.Structure):
+    _fields_ = [("krylov_dim", ctypes.c_int32), ("matvecs", ctypes.c_int32), ("seconds", ctypes.c_double)]
+
+
 class MinimumFamilyC(ctypes.Structure):
     _fields_ = [("id", ctypes.c_uint64), ("canonical_state", ctypes.c_uint64), ("sample_state", ctypes.c_uint64),
                 ("energy", ctypes.c_int64), ("times_visited", ctypes.c_uint64),
@@ -147,6 +157,10 @@ def load_library(build_if_missing=True):
                                     ctypes.c_int64, ctypes.POINTER(MinimumFamilyC), ctypes.c_int64, _i64p,
                                     ctypes.POINTER(CollectStatsC)]
     L.bk_adjoint.argtypes = [c_ctx, ctypes.POINTER(AdjointParamsC), _dp, _dp, _dp, ctypes.POINTER(AdjointStatsC)]
+    L.bk_fullspace_matvec.argtypes = [c_ctx, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_int]
+    L.bk_fullspace_lanczos.argtypes = [c_ctx, ctypes.POINTER(LanczosParamsC), _dp, _dp,
+                                       ctypes.POINTER(LanczosStatsC)]
     L.bk_sampler_run.argtypes = [c_ctx, ctypes.POINTER(SamplerConfigC), ctypes.c_uint64,
                                  ctypes.POINTER(SamplingResultC)]
     L.bk_sampling_result_release.argtypes = [ctypes.POINTER(SamplingResultC)]
@@ -396,6 +410,43 @@ class Engine:
         finally:
             if st == BK_OK:
                 self.L.bk_sampling_result_release(ctypes.byref(r))
+
+    def fullspace_matvec(self, n, g, x, y, scale=None, method=BK_FUSED):
+        """y = (scale E - g sum_j X_j) x on the device: x, y CUDA float64 tensors of 2^n
+        elements on this engine's device (scale defaults to 1/n, the reference's
+        normalize_by_n). method: BK_FUSED (tile passes) or BK_PLAIN (the reference's
+        one-thread-per-state form). Returns after the product is complete."""
+        import torch
+        for t in (x, y):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() == (1 << n)):
+                raise ValueError("x and y must be contiguous CUDA float64 tensors of 2^n elements")
+        torch.cuda.current_stream(x.device).synchronize()
+        self._check(self.L.bk_fullspace_matvec(self.ctx, n, g, (1.0 / n) if scale is None else scale,
+                                               ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                                               int(method)),
+                    "bk_fullspace_matvec")
+        return y
+
+    def fullspace_lanczos(self, n, g, num_eigenpairs=1, max_krylov_dim=100, tolerance=1e-12, normalize_by_n=True,
+                          vectors=True):
+        """The reference's Diagonalizer::solve_fullspace_lanczos (diagonalizer.cuh:377-560):
+        (energies[num_eigenpairs], vectors [num_eigenpairs, 2^n] or None, info) with the
+        tridiagonal matrix (alphas, betas) and the Krylov dimension reached in info."""
+        alphas = np.zeros(max(max_krylov_dim, 1))
+        betas = np.zeros(max(max_krylov_dim, 1))
+        prm = LanczosParamsC(n=n, g=g, num_eigenpairs=num_eigenpairs, max_krylov_dim=max_krylov_dim,
+                             tolerance=tolerance, normalize_by_n=int(bool(normalize_by_n)),
+                             alphas=_p(alphas, _dp), betas=_p(betas, _dp))
+        energies = np.zeros(num_eigenpairs)
+        vec = np.zeros((num_eigenpairs, 1 << n)) if vectors else None
+        st = LanczosStatsC()
+        self._check(self.L.bk_fullspace_lanczos(self.ctx, ctypes.byref(prm), _p(energies, _dp),
+                                                _p(vec, _dp) if vectors else None, ctypes.byref(st)),
+                    "bk_fullspace_lanczos")
+        m = st.krylov_dim
+        info = {"krylov_dim": m, "matvecs": st.matvecs, "seconds": st.seconds, "alphas": alphas[:m].copy(),
+                "betas": betas[:max(m - 1, 0)].copy()}
+        return energies, vec, info
 
     def export_state(self, n):
         out = np.empty(2 << n)

@@ -7,12 +7,14 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <iomanip>
 #include <iostream>
+#include <limits>
 #include <map>
 #include <random>
 #include <string>
@@ -24,6 +26,7 @@
 #include "bk_aux.cuh"
 #include "bk_engine.h"
 #include "bk_fused.cuh"
+#include "bk_lanczos.cuh"
 #include "bk_persist.cuh"
 
 using namespace bk;
@@ -109,6 +112,8 @@ struct bk_ctx {
   size_t adj_cap = 0;
   void* d_descent = nullptr;  // batched steepest descent: starts, final states, energies, evaluations
   size_t descent_cap = 0;
+  void* d_lz = nullptr;       // full-space Lanczos: Krylov basis, work vector, partial sums, alpha / beta
+  size_t lz_cap = 0;
   // last evolution (for export / sampling)
   bool have_state = false;
   bool last_planar = false;
@@ -1763,7 +1768,7 @@ int bk_destroy(bk_ctx* c) {
     if (p) cudaFree(p);
   for (auto& kv : c->batch_E) cudaFree(kv.second);
   for (void* p : {c->d_batch_state, c->d_batch, (void*)c->d_batch_results, c->d_persist, c->d_lam, c->d_ckpt,
-                  c->d_adj, c->d_descent})
+                  c->d_adj, c->d_descent, c->d_lz})
     if (p) cudaFree(p);
   for (auto& e : c->ev_pool) {
     cudaEventDestroy(e.first);
@@ -2583,3 +2588,264 @@ int bk_sample(bk_ctx* c, const double* randnums, int64_t shots, uint64_t* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Full-space Hamiltonian matvec and Lanczos (reference: src/subspace/diagonalizer.cuh
+// fullspace_matvec_kernel_d :60-77, solve_fullspace_lanczos :377-416,
+// run_gpu_lanczos_internal :418-560)
+// ---------------------------------------------------------------------------
+namespace {
+
+// n < 13: one CTA over the whole vector; else the block pass over index bits
+// [0, min(n, 23)) and, for n > 23, one strided tile pass over bits [23, n)
+// (w = n - 23 <= 7 bits, runs of 2^(13 - w) >= 64 doubles)
+int fs_matvec(bk_ctx* c, int n, double g, double scale, const double* x, double* y) {
+  BK_TRY(ensure_energy(c, n));
+  const int tile_bytes = (1 << kFsTileBits) * (int)sizeof(double);
+  size_t ev = 0;
+  BK_TRY(ev_begin(c, "fs_pass", &ev));
+  if (n < kFsTileBits) {
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(fs_pass_kernel), tile_bytes));
+    fs_pass_kernel<<<1, kFsThreads, (size_t)(1u << n) * sizeof(double), c->stream>>>(x, y, c->d_E, scale, g, n, n, n,
+                                                                                      0, 1, 0);
+    BK_CUDA(c, cudaGetLastError());
+    BK_TRY(ev_end(c, ev));
+    return BK_OK;
+  }
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(fs_block_kernel), tile_bytes));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(fs_tile_kernel), tile_bytes));
+  const uint32_t tiles = 1u << (n - kFsTileBits);
+  fs_block_kernel<<<tiles, kFsThreads, tile_bytes, c->stream>>>(x, y, c->d_E, scale, g, std::min(n, kFsGatherBits),
+                                                                c->d_err);
+  BK_CUDA(c, cudaGetLastError());
+  BK_TRY(ev_end(c, ev));
+  if (n > kFsGatherBits) {
+    const int w = n - kFsGatherBits, cp = kFsTileBits - w, h0 = kFsGatherBits;
+    BK_TRY(ev_begin(c, "fs_pass", &ev));
+    fs_tile_kernel<<<tiles, kFsThreads, tile_bytes, c->stream>>>(x, y, c->d_E, scale, g, cp, h0, h0 - cp, 0, cp,
+                                                                  c->d_err);
+    BK_CUDA(c, cudaGetLastError());
+    BK_TRY(ev_end(c, ev));
+  }
+  return BK_OK;
+}
+
+// the bounded waits' error word, cleared before and read after a full-space call
+int fs_err_clear(bk_ctx* c) {
+  BK_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+  return BK_OK;
+}
+int fs_err_check(bk_ctx* c) {
+  int e = 0;
+  BK_CUDA(c, cudaMemcpyAsync(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  BK_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (e != 0) return fail(c, BK_ERR_TIMEOUT, "fullspace matvec: a bounded device wait gave up (%d)", e);
+  return BK_OK;
+}
+
+// Eigenvalues (ascending) and eigenvectors of the symmetric tridiagonal matrix
+// with diagonal d[0..m) and off-diagonal e[0..m-1): the implicit QL algorithm
+// with Wilkinson shifts (Bowdler, Martin, Reinsch and Wilkinson, "The QR and QL
+// algorithms for symmetric matrices", Numer. Math. 11 (1968); EISPACK tql2).
+// z: m x m, column k = eigenvector k (row-major z[i * m + k]).
+bool tridiag_eigen(std::vector<double>& d, std::vector<double> e, std::vector<double>& z, int m) {
+  z.assign((size_t)m * m, 0.0);
+  for (int i = 0; i < m; ++i) z[(size_t)i * m + i] = 1.0;
+  e.resize((size_t)m, 0.0);
+  e[(size_t)m - 1] = 0.0;
+  const double eps = std::numeric_limits<double>::epsilon();
+  for (int l = 0; l < m; ++l) {
+    int iter = 0;
+    for (;;) {
+      int k = l;
+      for (; k < m - 1; ++k) {
+        const double dd = std::fabs(d[k]) + std::fabs(d[k + 1]);
+        if (std::fabs(e[k]) <= eps * dd) break;
+      }
+      if (k == l) break;
+      if (++iter > 60) return false;
+      // shift from the leading 2 x 2 block
+      double gq = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = std::hypot(gq, 1.0);
+      gq = d[k] - d[l] + e[l] / (gq + std::copysign(r, gq));
+      double sn = 1.0, cs = 1.0, pp = 0.0;
+      int i = k - 1;
+      bool deflated = false;
+      for (; i >= l; --i) {
+        const double f = sn * e[i], b = cs * e[i];
+        r = std::hypot(f, gq);
+        e[i + 1] = r;
+        if (r == 0.0) {
+          d[i + 1] -= pp;
+          e[k] = 0.0;
+          deflated = true;
+          break;
+        }
+        sn = f / r;
+        cs = gq / r;
+        gq = d[i + 1] - pp;
+        r = (d[i] - gq) * sn + 2.0 * cs * b;
+        pp = sn * r;
+        d[i + 1] = gq + pp;
+        gq = cs * r - b;
+        for (int row = 0; row < m; ++row) {
+          const double fz = z[(size_t)row * m + i + 1];
+          z[(size_t)row * m + i + 1] = sn * z[(size_t)row * m + i] + cs * fz;
+          z[(size_t)row * m + i] = cs * z[(size_t)row * m + i] - sn * fz;
+        }
+      }
+      if (deflated) continue;
+      d[l] -= pp;
+      e[l] = gq;
+      e[k] = 0.0;
+    }
+  }
+  // sort ascending with the vectors
+  std::vector<int> idx((size_t)m);
+  for (int i = 0; i < m; ++i) idx[(size_t)i] = i;
+  std::sort(idx.begin(), idx.end(), [&](int a, int b) { return d[(size_t)a] < d[(size_t)b]; });
+  std::vector<double> d2((size_t)m), z2((size_t)m * m);
+  for (int k = 0; k < m; ++k) {
+    d2[(size_t)k] = d[(size_t)idx[(size_t)k]];
+    for (int row = 0; row < m; ++row) z2[(size_t)row * m + k] = z[(size_t)row * m + idx[(size_t)k]];
+  }
+  d.swap(d2);
+  z.swap(z2);
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bk_fullspace_matvec(bk_ctx* c, int n, double g, double scale, const double* d_x, double* d_y, int method) {
+  if (!c || !d_x || !d_y) return BK_ERR_INVALID;
+  if (method != BK_FUSED && method != BK_PLAIN) return fail(c, BK_ERR_INVALID, "fullspace matvec: method %d", method);
+  if (n < 1 || n > kMaxN) return fail(c, BK_ERR_UNSUPPORTED, "n = %d outside [1, %d]", n, kMaxN);
+  if (d_x == d_y) return fail(c, BK_ERR_INVALID, "fullspace matvec: x and y must not alias");
+  if ((reinterpret_cast<uintptr_t>(d_x) | reinterpret_cast<uintptr_t>(d_y)) & 15u)
+    return fail(c, BK_ERR_INVALID, "fullspace matvec: x and y must be 16-byte aligned (bulk copies)");
+  BK_CUDA(c, cudaSetDevice(c->device));
+  BK_TRY(fs_err_clear(c));
+  if (method == BK_PLAIN) {
+    BK_TRY(ensure_energy(c, n));
+    const uint64_t N = 1ull << n;
+    size_t ev = 0;
+    BK_TRY(ev_begin(c, "fs_plain", &ev));
+    fs_plain_kernel<<<(unsigned)((N + 255) / 256), 256, 0, c->stream>>>(d_x, d_y, c->d_E, scale, g, n, N);
+    BK_CUDA(c, cudaGetLastError());
+    BK_TRY(ev_end(c, ev));
+  } else {
+    BK_TRY(fs_matvec(c, n, g, scale, d_x, d_y));
+  }
+  BK_TRY(fs_err_check(c));
+  BK_TRY(collect_timing(c));
+  return BK_OK;
+}
+
+int bk_fullspace_lanczos(bk_ctx* c, const bk_lanczos_params* p, double* energies, double* vectors,
+                         bk_lanczos_stats* stats) {
+  if (!c || !p || !energies) return BK_ERR_INVALID;
+  const int n = p->n;
+  if (n < 1 || n > kMaxN) return fail(c, BK_ERR_UNSUPPORTED, "n = %d outside [1, %d]", n, kMaxN);
+  if (p->num_eigenpairs < 1 || p->max_krylov_dim < 1)
+    return fail(c, BK_ERR_INVALID, "lanczos: num_eigenpairs and max_krylov_dim must be >= 1");
+  BK_CUDA(c, cudaSetDevice(c->device));
+  cudaStream_t st = c->stream;
+  const uint64_t N = 1ull << n;
+  const int m = (int)std::min<uint64_t>(N, (uint64_t)p->max_krylov_dim);
+  const double scale = p->normalize_by_n ? (1.0 / static_cast<double>(n)) : 1.0;
+  // Krylov basis V[m][N], work vector w, partial sums, alpha[m], beta[m], norm
+  const size_t need = ((size_t)m + 1) * N * sizeof(double) + (kLzBlocks + 2 * (size_t)m + 8) * sizeof(double);
+  if (c->lz_cap < need) {
+    // the old buffer is released before the new one is taken; keep 256 MB of headroom
+    size_t free_b = 0, total_b = 0;
+    BK_CUDA(c, cudaMemGetInfo(&free_b, &total_b));
+    if (need + (256ull << 20) > free_b + c->lz_cap)
+      return fail(c, BK_ERR_UNSUPPORTED, "lanczos: %d Krylov vectors of 2^%d doubles need %.1f GB (%.1f GB free)",
+                  m + 1, n, need / 1e9, (free_b + c->lz_cap) / 1e9);
+  }
+  BK_TRY(ensure_buffer(c, &c->d_lz, &c->lz_cap, need));
+  double* V = static_cast<double*>(c->d_lz);
+  double* w = V + (size_t)m * N;
+  double* partials = w + N;
+  double* d_alpha = partials + kLzBlocks;
+  double* d_beta = d_alpha + m;
+  double* d_norm = d_beta + m;
+  BK_TRY(ensure_energy(c, n));
+  BK_TRY(fs_err_clear(c));
+  auto t0 = std::chrono::steady_clock::now();
+  // start vector: the reference's mt19937_64(42), uniform on (-0.5, 0.5) (diagonalizer.cuh:433-437)
+  {
+    std::mt19937_64 rng(42);
+    std::uniform_real_distribution<double> dist(-0.5, 0.5);
+    std::vector<double> v0(N);
+    for (uint64_t i = 0; i < N; ++i) v0[i] = dist(rng);
+    BK_CUDA(c, cudaMemcpyAsync(V, v0.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+    BK_CUDA(c, cudaStreamSynchronize(st));
+  }
+  const unsigned eg = kLzBlocks;
+  lz_axpy_nrm_kernel<<<eg, 256, 0, st>>>(V, V, d_alpha, -1, N, partials);
+  lz_reduce_kernel<<<1, 256, 0, st>>>(partials, (int)eg, d_norm, 0, 1);
+  lz_scale_kernel<<<eg, 256, 0, st>>>(V, V, d_norm, 0, N);
+  BK_CUDA(c, cudaGetLastError());
+  int m_actual = m, matvecs = 0;
+  std::vector<double> h_alpha((size_t)m, 0.0), h_beta((size_t)m, 0.0);
+  for (int j = 0; j < m; ++j) {
+    double* vj = V + (size_t)j * N;
+    BK_TRY(fs_matvec(c, n, p->g, scale, vj, w));
+    ++matvecs;
+    lz_orth_dot_kernel<<<eg, 256, 0, st>>>(w, j > 0 ? vj - N : vj, vj, d_beta, j - 1, N, partials);
+    lz_reduce_kernel<<<1, 256, 0, st>>>(partials, (int)eg, d_alpha, j, 0);
+    if (j < m - 1) {
+      lz_axpy_nrm_kernel<<<eg, 256, 0, st>>>(w, vj, d_alpha, j, N, partials);
+      lz_reduce_kernel<<<1, 256, 0, st>>>(partials, (int)eg, d_beta, j, 1);
+      BK_CUDA(c, cudaGetLastError());
+      BK_CUDA(c, cudaMemcpyAsync(&h_beta[(size_t)j], d_beta + j, sizeof(double), cudaMemcpyDeviceToHost, st));
+      BK_CUDA(c, cudaStreamSynchronize(st));
+      if (std::fabs(h_beta[(size_t)j]) < p->tolerance) {  // breakdown (diagonalizer.cuh:463-466)
+        m_actual = j + 1;
+        break;
+      }
+      lz_scale_kernel<<<eg, 256, 0, st>>>(vj + N, w, d_beta, j, N);
+    }
+    BK_CUDA(c, cudaGetLastError());
+  }
+  BK_CUDA(c, cudaMemcpyAsync(h_alpha.data(), d_alpha, (size_t)m_actual * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (m_actual > 1)
+    BK_CUDA(c, cudaMemcpyAsync(h_beta.data(), d_beta, (size_t)(m_actual - 1) * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
+  BK_CUDA(c, cudaStreamSynchronize(st));
+  BK_TRY(fs_err_check(c));
+  BK_TRY(collect_timing(c));
+  std::vector<double> dvals(h_alpha.begin(), h_alpha.begin() + m_actual);
+  std::vector<double> evals(h_beta.begin(), h_beta.begin() + std::max(m_actual - 1, 0));
+  std::vector<double> z;
+  if (!tridiag_eigen(dvals, evals, z, m_actual))
+    return fail(c, BK_ERR_CUDA, "lanczos: the tridiagonal eigensolver did not converge");
+  const int k_pairs = std::min(p->num_eigenpairs, m_actual);
+  for (int k = 0; k < p->num_eigenpairs; ++k) energies[k] = k < k_pairs ? dvals[(size_t)k] : std::nan("");
+  if (vectors) {
+    // Ritz vectors x_k = V y_k (diagonalizer.cuh:526-538)
+    std::vector<double> coef((size_t)m_actual);
+    for (int k = 0; k < k_pairs; ++k) {
+      for (int j = 0; j < m_actual; ++j) coef[(size_t)j] = z[(size_t)j * m_actual + k];
+      BK_CUDA(c, cudaMemcpyAsync(partials, coef.data(), (size_t)m_actual * sizeof(double), cudaMemcpyHostToDevice, st));
+      lz_combine_kernel<<<eg, 256, 0, st>>>(V, partials, m_actual, N, w);
+      BK_CUDA(c, cudaGetLastError());
+      BK_CUDA(c, cudaMemcpyAsync(vectors + (size_t)k * N, w, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    BK_CUDA(c, cudaStreamSynchronize(st));
+  }
+  if (p->alphas) std::copy(h_alpha.begin(), h_alpha.begin() + m_actual, p->alphas);
+  if (p->betas) std::copy(h_beta.begin(), h_beta.begin() + std::max(m_actual - 1, 0), p->betas);
+  if (stats) {
+    stats->krylov_dim = m_actual;
+    stats->matvecs = matvecs;
+    stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return BK_OK;
+}
+
+}  // extern "C"
+

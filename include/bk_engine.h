@@ -365,6 +365,43 @@ int bk_sample(bk_ctx* ctx, const double* randnums, int64_t shots, uint64_t* out_
 int bk_measure_noalloc(int n, int precision, const void* d_state, int64_t e0, uint64_t s0, double* d_out,
                        void* stream);
 
+/* ---- full-space Hamiltonian (H = diag(scale E(s)) - g sum_j X_j, all 2^n states, FP64) ----
+ *
+ * bk_fullspace_matvec: y = H x for device vectors of 2^n doubles (replaces the
+ * reference's fullspace_matvec_kernel_d, src/subspace/diagonalizer.cuh:60-77, with
+ * diag = scale * E(s) as in :388-392). x and y are 16-byte aligned device pointers on
+ * the context's device and must not alias; the call runs on the context's stream and returns
+ * after it has finished (the caller's own work on x must be complete before).
+ * method: BK_FUSED = tile passes over 64 KB shared-memory tiles (x read once per
+ * pass), BK_PLAIN = the reference's one-thread-per-state form (comparison).
+ *
+ * bk_fullspace_lanczos: the reference's Diagonalizer::solve_fullspace_lanczos
+ * (diagonalizer.cuh:377-416 with run_gpu_lanczos_internal :418-560): plain Lanczos
+ * from the start vector mt19937_64(42) / uniform(-0.5, 0.5), m = min(2^n,
+ * max_krylov_dim) steps, stopping when beta < tolerance; the lowest
+ * num_eigenpairs Ritz values in energies (NaN beyond the Krylov dimension) and,
+ * when vectors != NULL, their Ritz vectors ([num_eigenpairs][2^n] doubles, host).
+ * alphas / betas (optional, host, max_krylov_dim entries) receive the tridiagonal
+ * matrix. Needs (m + 1) 2^n doubles of device memory (BK_ERR_UNSUPPORTED if not free). */
+typedef struct bk_lanczos_params {
+  int n;
+  double g;
+  int num_eigenpairs;  /* reference default 1 */
+  int max_krylov_dim;  /* reference default 100 */
+  double tolerance;    /* reference default 1e-12 */
+  int normalize_by_n;  /* reference default 1: diagonal E / n */
+  double* alphas;      /* optional out [max_krylov_dim] */
+  double* betas;       /* optional out [max_krylov_dim] */
+} bk_lanczos_params;
+typedef struct bk_lanczos_stats {
+  int krylov_dim;      /* steps taken (m_actual) */
+  int matvecs;
+  double seconds;      /* wall time of the run, start vector included */
+} bk_lanczos_stats;
+int bk_fullspace_matvec(bk_ctx* ctx, int n, double g, double scale, const double* d_x, double* d_y, int method);
+int bk_fullspace_lanczos(bk_ctx* ctx, const bk_lanczos_params* params, double* energies, double* vectors,
+                         bk_lanczos_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

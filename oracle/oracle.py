@@ -244,3 +244,30 @@ def sampler_run(cfg: dict, start_bits: int) -> dict:
                               mean_hamming_flips=float(sd["seed_mean_hamming"][i]),
                               best_energy=int(sbe[i])) for i in range(ns)]
     return out
+
+
+def fullspace_matvec(n, g, x, scale=None, threads=0):
+    """y = (scale E - g sum_j X_j) x, the reference's per-state order (diagonalizer.cuh:60-77)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L = lib()
+    L.orc_fullspace_matvec.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp, ctypes.c_int]
+    if L.orc_fullspace_matvec(n, g, (1.0 / n) if scale is None else scale, _ptr(x, dp), _ptr(y, dp), threads):
+        raise ValueError("orc_fullspace_matvec rejected its arguments")
+    return y
+
+
+def fullspace_lanczos(n, g, max_krylov_dim=100, tolerance=1e-12, normalize_by_n=True, threads=0):
+    """The reference's plain Lanczos (diagonalizer.cuh:418-482) on the CPU: (alphas, betas)."""
+    dp = ctypes.POINTER(ctypes.c_double)
+    L = lib()
+    L.orc_fullspace_lanczos.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                        ctypes.c_double, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    a = np.zeros(max(max_krylov_dim, 1))
+    b = np.zeros(max(max_krylov_dim, 1))
+    m = ctypes.c_int(0)
+    if L.orc_fullspace_lanczos(n, g, (1.0 / n) if normalize_by_n else 1.0, max_krylov_dim, tolerance, _ptr(a, dp),
+                               _ptr(b, dp), ctypes.byref(m), threads):
+        raise ValueError("orc_fullspace_lanczos rejected its arguments")
+    return a[:m.value].copy(), b[:max(m.value - 1, 0)].copy()

@@ -679,3 +679,80 @@ int orc_sampler_run(const orc_sampler_config* cfg, uint64_t start_bits, orc_samp
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Full-space Hamiltonian H = diag(scale E(s)) - g sum_j X_j and the plain
+// Lanczos iteration over it (src/subspace/diagonalizer.cuh).
+// ---------------------------------------------------------------------------
+namespace {
+
+// y = H x, each state in the reference's order: diag * x_i, then - g x[i ^ 2^j]
+// for j = 0..n-1 (fullspace_matvec_kernel_d, diagonalizer.cuh:60-77; the
+// diagonal scale * E(s), :388-392)
+void fs_matvec(int n, double g, double scale, const double* x, double* y) {
+  const int64_t dim = int64_t(1) << n;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < dim; ++i) {
+    double yi = static_cast<double>(energy_of(n, static_cast<uint64_t>(i))) * scale * x[i];
+    for (int j = 0; j < n; ++j) yi -= g * x[i ^ (int64_t(1) << j)];
+    y[i] = yi;
+  }
+}
+
+double dot(const std::vector<double>& a, const std::vector<double>& b) {
+  double s = 0.0;
+  for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+  return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_fullspace_matvec(int n, double g, double scale, const double* x, double* y, int n_threads) {
+  if (n < 1 || n > 26 || !x || !y) return 1;
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+  fs_matvec(n, g, scale, x, y);
+  return 0;
+}
+
+// The reference's run_gpu_lanczos_internal (diagonalizer.cuh:418-482) in FP64 on
+// the CPU: start vector mt19937_64(42) / uniform(-0.5, 0.5) normalised; per step
+// w = H v_j, w -= beta_{j-1} v_{j-1}, alpha_j = v_j . w, w -= alpha_j v_j, and
+// (j < m - 1) beta_j = |w|, stop when beta_j < tol, v_{j+1} = w / beta_j.
+// alphas[m_actual], betas[m_actual - 1]; *m_actual = steps taken.
+int orc_fullspace_lanczos(int n, double g, double scale, int max_krylov_dim, double tol, double* alphas,
+                          double* betas, int* m_actual, int n_threads) {
+  if (n < 1 || n > 24 || max_krylov_dim < 1 || !alphas || !betas || !m_actual) return 1;
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+  const int64_t N = int64_t(1) << n;
+  const int m = static_cast<int>(std::min<int64_t>(N, max_krylov_dim));
+  std::vector<double> v(N), vprev(N, 0.0), w(N);
+  std::mt19937_64 rng(42);
+  std::uniform_real_distribution<double> dist(-0.5, 0.5);
+  for (int64_t i = 0; i < N; ++i) v[i] = dist(rng);
+  const double inv0 = 1.0 / std::sqrt(dot(v, v));
+  for (auto& a : v) a *= inv0;
+  int mm = m;
+  for (int j = 0; j < m; ++j) {
+    fs_matvec(n, g, scale, v.data(), w.data());
+    if (j > 0)
+      for (int64_t i = 0; i < N; ++i) w[i] -= betas[j - 1] * vprev[i];
+    alphas[j] = dot(v, w);
+    for (int64_t i = 0; i < N; ++i) w[i] -= alphas[j] * v[i];
+    if (j < m - 1) {
+      betas[j] = std::sqrt(dot(w, w));
+      if (std::fabs(betas[j]) < tol) {
+        mm = j + 1;
+        break;
+      }
+      const double inv = 1.0 / betas[j];
+      vprev.swap(v);
+      for (int64_t i = 0; i < N; ++i) v[i] = w[i] * inv;
+    }
+  }
+  *m_actual = mm;
+  return 0;
+}
+
+}  // extern "C"
