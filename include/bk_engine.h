@@ -380,7 +380,8 @@ int bk_measure_noalloc(int n, int precision, const void* d_state, int64_t e0, ui
  * from the start vector mt19937_64(42) / uniform(-0.5, 0.5), m = min(2^n,
  * max_krylov_dim) steps, stopping when beta < tolerance; the lowest
  * num_eigenpairs Ritz values in energies (NaN beyond the Krylov dimension) and,
- * when vectors != NULL, their Ritz vectors ([num_eigenpairs][2^n] doubles, host).
+ * when vectors != NULL, their Ritz vectors ([num_eigenpairs][2^n] doubles, host;
+ * rows beyond the Krylov dimension are left as the caller allocated them).
  * alphas / betas (optional, host, max_krylov_dim entries) receive the tridiagonal
  * matrix. Needs (m + 1) 2^n doubles of device memory (BK_ERR_UNSUPPORTED if not free). */
 typedef struct bk_lanczos_params {
