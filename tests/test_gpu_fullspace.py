@@ -95,3 +95,21 @@ def test_fullspace_errors(eng):
         eng.fullspace_lanczos(28, 0.3, max_krylov_dim=500, vectors=False)  # 501 x 2 GB does not fit
     e, _, info = eng.fullspace_lanczos(3, 0.3, num_eigenpairs=10, vectors=False)  # m = min(2^n, 100) = 8
     assert info["krylov_dim"] <= 8 and np.isnan(e[-1])
+
+
+def test_reference_lanczos_known_answer(eng):
+    """The reference's own check (tests/test_lanczos.cu:10-59): n = 4, g = 0.5,
+    max_krylov_dim 30 (the whole 16-state space): ground energy within 1e-6 of
+    dense ED and ||H v - E v|| < 1e-5."""
+    n, g = 4, 0.5
+    e, vec, info = eng.fullspace_lanczos(n, g, max_krylov_dim=30)
+    N = 1 << n
+    E = np.array(bk.labs_energy(n, np.arange(N, dtype=np.uint64)), dtype=np.float64)
+    H = np.diag(E / n)
+    idx = np.arange(N)
+    for j in range(n):
+        H[idx, idx ^ (1 << j)] -= g
+    assert info["krylov_dim"] <= N
+    assert abs(e[0] - np.linalg.eigvalsh(H)[0]) < 1e-6
+    v = vec[0]
+    assert np.linalg.norm(H @ v - e[0] * v) < 1e-5
