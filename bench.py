@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--a1-kernel", type=int, default=None, choices=[0, 1, 2],
                     help="per-pass A1 kernel: 0 = 256x16, 1 = 512x8, 2 = warp-local (element bits 0-8)")
     ap.add_argument("--no-tune", action="store_true", help="engine defaults instead of the autotuner's choice")
+    ap.add_argument("--kernel-table-steps", type=int, default=3,
+                    help="bench steps of the separate per-kernel timing pass (roofline)")
     return ap.parse_args()
 
 
@@ -136,11 +138,28 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def large_config(a, n, bits, e0, seed, world=1):
+    """The workload of the N = 28 headline line, shared by both arms so the
+    driver compares like with like."""
+    S = 8 if a.precision == "c64" else 16
+    return {"workload": f"N={n} single trap (lowest 1% of 4000 descents, seed {seed}), g={a.g}, dt={a.dt}, "
+                        f"{a.trotter} Trotter steps per bench step, P_< and <d_H> every {a.measure_every} steps",
+            "n": n, "trap_bits": hex(bits), "trap_energy": int(e0), "trotter_steps_per_step": a.trotter,
+            "l2": f"state {((1 << n) * S) / 2**30:.1f} GiB > 126 MB L2, no flush needed",
+            "parallelism": f"replicas x{world}"}
+
+
+def oracle_trap(n, seed=42):
+    """The benchmark trap selected by the oracle (the reference's compiled descent
+    when oracle/_ref was built): the CPU legs never load the product library."""
+    from oracle import oracle as O
+    return O.select_trap(n, seed, 4000 if n >= 28 else 1000, 0.01 if n >= 28 else 0.05)
+
+
 def cpu_baseline(n, steps, g, dt):
     """The oracle's complex128 per-qubit restatement of the reference step, all host threads."""
     from oracle import oracle as O
-    import bk_b200 as bk
-    bits, e0 = bk.select_trap(n, 42, 4000 if n >= 28 else 1000, 0.01 if n >= 28 else 0.05)
+    bits, e0 = oracle_trap(n)
     secs = np.zeros(steps)
     threads = os.cpu_count() or 1
     O.trotter_evolve(n, bits, e0, g, dt, steps, measure=[0], threads=threads, step_seconds=secs)
@@ -172,9 +191,8 @@ def run_reference(a):
     if rank != 0:
         return
     from oracle import oracle as O
-    import bk_b200 as bk
     n = a.n
-    bits, e0 = bk.select_trap(n, 42, 4000 if n >= 28 else 1000, 0.01 if n >= 28 else 0.05)
+    bits, e0 = oracle_trap(n)
     total = a.warmup + a.steps
     secs = np.zeros(total)
     threads = os.cpu_count() or 1
@@ -186,14 +204,38 @@ def run_reference(a):
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * float(timed.mean()),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic (seeded trap from 4000 steepest descents, no dataset)",
-            "config": {"workload": f"N={n} single trap, g={a.g}, dt={a.dt}, 1 Trotter step per bench step, "
-                                   f"P_< and <d_H> every {a.measure_every} steps", "n": n,
-                       "trap_bits": hex(bits), "trap_energy": e0},
+            "config": large_config(a, n, bits, e0, 42, a.gpus),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{total} Trotter steps of the N={n} trap (oracle complex128 restatement of "
-                                       f"the reference's phase + per-qubit Rx loop), timed per step"},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": f"a bounded sample of the workload: {total} Trotter steps of the same N={n} "
+                                       f"trap ({a.warmup} untimed), one per bench step, P_< and <d_H> every "
+                                       f"{a.measure_every} steps, by the oracle's complex128 restatement of the "
+                                       f"reference's phase + per-qubit Rx loop on all host threads"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "custatevec": custatevec_probe()}
     print(json.dumps(line))
+
+
+def custatevec_probe():
+    """Whether the reference's own GPU path (cuStateVec, sampler.cuh:412-707) could
+    run on this machine: the cuquantum Python package or a libcustatevec the
+    loader can find. The reference sampler also needs custatevec.h to build."""
+    import ctypes.util
+    found = []
+    try:
+        import cuquantum  # noqa: F401
+        found.append("python package cuquantum")
+    except Exception:
+        pass
+    lib = ctypes.util.find_library("custatevec")
+    if lib:
+        found.append(lib)
+    hdr = [d for d in ("/usr/include", "/usr/local/include", "/usr/local/cuda/include")
+           if os.path.exists(os.path.join(d, "custatevec.h"))]
+    if found and hdr:
+        return {"available": True, "found": found + hdr}
+    return {"available": False,
+            "detail": "unavailable on this box: " + ("; ".join(found) if found else "no cuquantum package, no "
+                      "libcustatevec") + ("" if hdr else ", no custatevec.h")}
 
 
 def replica_trap(n, rank, n_descents=4000, quantile=0.01):
@@ -293,6 +335,18 @@ def run_batched(a):
         seq["sequential_" + ("one_launch_per_pass" if mode == 1 else "persistent_per_instance")] = \
             amp_steps / (e0_.elapsed_time(e1_) / 1e3)
     best_seq = max(seq.values())
+    # roofline: one persistent launch per bench step runs all 500 steps of all
+    # 512 instances; algorithmic bytes 32 per amplitude-step (two complex64
+    # read + write passes), timed by the CUDA events bracketing the launches
+    peak, peak_kind = measured_peaks()
+    launch_s = dev_s / a.steps
+    alg = 32.0 * amp_steps
+    roof = {"bound": "hbm", "kernel": "persist_kernel (batched, one graph launch per bench step)",
+            "achieved": alg / launch_s / 1e9, "peak": peak, "unit": "GB/s", "frac": alg / launch_s / 1e9 / peak,
+            "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg, "avg_launch_ms": 1e3 * launch_s,
+            "traffic": None,
+            "l2": "each statevector is 0.5-32 MiB (N = 16-22, complex64); the tasks of a few statevectors in flight "
+                  "fit the 126 MB L2, so part of the traffic is served from L2 and the HBM fraction is nominal"}
     line = {"metric": "Batched Trotter amp-steps/s (512 instances, N in {16,18,20,22}, complex64)", "value": value,
             "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * dev_s / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -308,10 +362,32 @@ def run_batched(a):
             "compare": dict(seq, batched_over_best_sequential=value / best_seq),
             "e2e": {"value": amp_steps * a.steps / wall, "unit": UNIT, "h2d_bytes_per_step": 24 * len(inst) + 501,
                     "d2h_bytes_per_step": 3 * 8 * len(inst) * 501},
-            "clocks": clocks.summary(),
+            "clocks": clocks.summary(), "roofline": roof, "gpu_launches": a.steps,
             "check": {"p_less_mean_last": float(np.mean(p[:, -1])), "norm_max_dev": float(np.max(np.abs(nn - 1)))}}
     eng.close()
+    if not a.no_cpu_baseline:
+        line["cpu_baseline"] = batched_cpu_baseline(inst, a.dt)
     print(json.dumps(line))
+
+
+def batched_cpu_baseline(inst, dt, per_n=2, steps=10):
+    """The oracle's complex128 restatement on the same instance mix, sampled:
+    `per_n` instances of each N in the batch, `steps` Trotter steps each, all host threads."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    picked, seen = [], {}
+    for d in inst:
+        if seen.get(d["n"], 0) < per_n:
+            seen[d["n"]] = seen.get(d["n"], 0) + 1
+            picked.append(d)
+    amp, t0 = 0.0, time.perf_counter()
+    for d in picked:
+        O.trotter_evolve(d["n"], d["s0"], d["e0"], d["g"], dt, steps, measure=[0], threads=threads)
+        amp += float(1 << d["n"]) * steps
+    secs = time.perf_counter() - t0
+    return {"value": amp / secs, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(picked)} instances of the batch ({per_n} per N in {sorted(seen)}), {steps} Trotter steps "
+                      f"each, oracle complex128 restatement (phase + per-qubit Rx), {secs:.1f} s"}
 
 
 def run_adjoint(a):
@@ -352,6 +428,29 @@ def run_adjoint(a):
     torch.cuda.synchronize(dev)
     fwd_s = f0.elapsed_time(f1) / 1e3 / a.steps
     amp_steps = float(1 << n) * T
+    # roofline of the reverse sweep (the dominant part): per amplitude-step it
+    # reads and writes psi and lambda in two passes, 8 S bytes (S = 8 complex64, 16 complex128)
+    S = 8 if prec == bk.BK_C64 else 16
+    peak, peak_kind = measured_peaks()
+    rev_s = float(np.mean(rv)) / 1e3
+    alg = 8.0 * S * amp_steps
+    roof = {"bound": "hbm", "kernel": "adjoint reverse sweep (dual-state tile passes)",
+            "achieved": alg / rev_s / 1e9, "peak": peak, "unit": "GB/s", "frac": alg / rev_s / 1e9 / peak,
+            "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg, "avg_launch_ms": 1e3 * rev_s,
+            "traffic": None,
+            "l2": "psi and lambda are 32 MiB each at N = 22 complex64: both fit the 126 MB L2, so the HBM "
+                  "fraction is nominal"}
+    cpu = None
+    if not a.no_cpu_baseline:
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        Tc = 20
+        t0c = time.perf_counter()
+        O.trotter_adjoint(n, bits, e0, g_steps[:Tc], a.dt, Tc, threads=threads)
+        secs = time.perf_counter() - t0c
+        cpu = {"value": float(1 << n) * Tc / secs, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"forward + adjoint gradient of {Tc} steps of the same N=22 trap and schedule by the "
+                         f"oracle (complex128, exact gates, sqrt(T) checkpoints), {secs:.1f} s"}
     line = {"metric": "Adjoint gradient amp-steps/s (N=22, 64 segments, 1280 steps; forward + reverse sweep)",
             "value": amp_steps * a.steps / dev_s, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * dev_s / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -366,7 +465,8 @@ def run_adjoint(a):
                         "max_checkpoint_drift": st["max_drift"]},
             "e2e": {"value": amp_steps * a.steps / wall, "unit": UNIT, "h2d_bytes_per_step": 8 * nseg + 96,
                     "d2h_bytes_per_step": 8 * (nseg + 1 + T)},
-            "clocks": clocks.summary(), "check": {"p_less_T": val, "grad_max_abs": float(np.max(np.abs(grad)))}}
+            "clocks": clocks.summary(), "roofline": roof, "cpu_baseline": cpu,
+            "check": {"p_less_T": val, "grad_max_abs": float(np.max(np.abs(grad)))}}
     eng.close()
     print(json.dumps(line))
 
@@ -437,8 +537,10 @@ def run_matvec(a):
             "config": {"workload": f"y = (E/N) x - 0.35 sum_j x[i ^ 2^j] over 2^{n} states, FP64, 10 products per "
                                    "bench step", "n": n, "products_per_step": reps,
                        "l2": f"x and y {8 * states / 2**30:.1f} GiB each > 126 MB L2, no flush needed",
-                       "passes": "pass 0 over index bits 0-12, then strided passes of <= 9 bits",
-                       "design_dram_bytes_per_state": 66},
+                       "passes": "block pass over 8192-state blocks (index bits 0-12 in shared memory, bits 13-22 "
+                                 "as L2 sweeps of partner blocks), then for n > 23 one strided tile pass over "
+                                 "bits [23, n)",
+                       "design_dram_bytes_per_state": 42},
             "roofline": {"bound": "hbm", "kernel": "fs_pass (all passes of one product)", "achieved": alg / per / 1e9,
                          "peak": peak, "unit": "GB/s", "frac": alg / per / 1e9 / peak, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg, "avg_launch_ms": 1e3 * per, "traffic": None,
@@ -501,10 +603,9 @@ def main():
     for _ in range(max(a.warmup, 0)):
         bench_step()
 
-    # ---- device-timed region (value + live per-kernel timing) ----
+    # ---- device-timed region (value): the production path, no per-launch events ----
     barrier()
     torch.cuda.synchronize(dev)
-    eng.set_kernel_timing(True)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
@@ -515,9 +616,18 @@ def main():
         torch.cuda.synchronize(dev)
     barrier()
     dev_s = ev0.elapsed_time(ev1) / 1e3
+    dev_s_max = max_over_ranks(dev_s, world, f"cuda:{local}")
+
+    # ---- per-kernel table for the roofline: a separate pass with CUDA events
+    # around every launch (outside the timed region above) ----
+    barrier()
+    eng.set_kernel_timing(True)
+    for _ in range(min(a.steps, a.kernel_table_steps)):
+        bench_step()
+    torch.cuda.synchronize(dev)
     timing = eng.kernel_timing()
     eng.set_kernel_timing(False)
-    dev_s_max = max_over_ranks(dev_s, world, f"cuda:{local}")
+    barrier()
 
     # ---- end-to-end region: the C-ABI call with host buffers, wall clock ----
     barrier()
@@ -546,23 +656,23 @@ def main():
     achieved = abytes / (dms / dl / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = committed_traffic().get(f"{dname}/n{n}/{a.precision}")
-    launches = sum(v[0] for v in timing.values()) + a.steps  # + one basis-state init per call
+    # launches per bench step from the timing pass, scaled to the timed steps
+    # (+ one basis-state init per call)
+    table_steps = max(1, min(a.steps, a.kernel_table_steps))
+    launches = int(round(sum(v[0] for v in timing.values()) * a.steps / table_steps)) + a.steps
 
     line = {"metric": METRIC.format(n=n), "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1e3 * dev_s_max / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64" if prec == bk.BK_C64 else "c128",
             "data": "synthetic (seeded trap from 4000 steepest descents, no dataset)",
-            "config": {"workload": f"N={n} single trap (lowest 1% of 4000 descents, seed {42 + rank}), g={a.g}, "
-                                   f"dt={a.dt}, {T} Trotter steps per bench step, P_< and <d_H> every "
-                                   f"{a.measure_every} steps, {a.precision} fused",
-                       "n": n, "trap_bits": hex(bits), "trap_energy": e0, "trotter_steps_per_step": T,
-                       "l2": f"state {((1 << n) * S) / 2**30:.1f} GiB > 126 MB L2, no flush needed",
-                       "parallelism": f"replicas x{world}", "tuning": tuning},
+            "config": large_config(a, n, bits, e0, 42 + rank, world), "tuning": tuning,
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": dms / dl,
                          "traffic": traffic},
             "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 3)} for k, v in timing.items()},
+            "kernel_table": f"{table_steps} bench steps with CUDA events around every launch, after the timed "
+                            "region (the timed region runs without them)",
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * 8 + (T + 1),
                     "d2h_bytes_per_step": 8 * 3 * len(meas) + 8 * 4 * len(meas)},
             "gpu_launches": launches, "clocks": clocks.summary(),
@@ -575,22 +685,34 @@ def main():
         # the complex128 runs use complex128's own tuned knobs (else the engine defaults)
         if tune.apply(eng, n, bk.BK_C128) is None:
             tune.apply_config(eng, tune.DEFAULTS)
-        for name, pr, meth, steps in (("c128_fused", bk.BK_C128, bk.BK_FUSED, 40),
+        c128_series = None
+        for name, pr, meth, steps in (("c128_fused", bk.BK_C128, bk.BK_FUSED, T),
                                       ("c128_plain", bk.BK_C128, bk.BK_PLAIN, 20)):
             eng.evolve(n, bits, a.g, a.dt, 2, measure=[0], e0=e0, precision=pr, method=meth)
             torch.cuda.synchronize(dev)
             e0_ = torch.cuda.Event(enable_timing=True)
             e1_ = torch.cuda.Event(enable_timing=True)
             e0_.record(stream)
-            eng.evolve(n, bits, a.g, a.dt, steps, measure=list(range(0, steps + 1, a.measure_every)), e0=e0,
-                       precision=pr, method=meth)
+            out = eng.evolve(n, bits, a.g, a.dt, steps, measure=list(range(0, steps + 1, a.measure_every)), e0=e0,
+                             precision=pr, method=meth)
             e1_.record(stream)
             torch.cuda.synchronize(dev)
             cmp[name] = float(1 << n) * steps / (e0_.elapsed_time(e1_) / 1e3)
+            if name == "c128_fused":
+                c128_series = out
         cmp["c64_fused"] = value
         cmp["c64_fused_over_c128_plain"] = value / cmp["c128_plain"]
         cmp["c64_fused_over_c128_fused"] = value / cmp["c128_fused"]
+        cmp["custatevec"] = custatevec_probe()
         line["compare"] = cmp
+        if prec == bk.BK_C64 and c128_series is not None:
+            # the bench step's own series (c64, tuned knobs) against complex128 on the same trap and schedule
+            p128, d128, _ = c128_series
+            line["check"]["c64_vs_c128"] = {
+                "trotter_steps": T, "points": len(meas),
+                "max_abs_dP_less": float(np.max(np.abs(p_last - p128))),
+                "max_abs_d_dH": float(np.max(np.abs(d_last - d128))),
+                "bar_dP_less": 1e-6}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(n, a.cpu_baseline_steps, a.g, a.dt)

@@ -459,7 +459,8 @@ class Engine:
         self._check(self.L.bk_sample(self.ctx, _p(r, _dp), len(r), _p(out, _u64p)), "bk_sample")
         return out
 
-    OPTIONS = {"engine_mode": 0, "slab_lag": 1, "split_w2": 2, "e_source": 3, "a1_wide": 4, "adj_a1": 5}
+    OPTIONS = {"engine_mode": 0, "slab_lag": 1, "split_w2": 2, "e_source": 3, "a1_wide": 4, "adj_a1": 5,
+               "wait_polls": 6, "test_hold_step": 7}
 
     def set_option(self, name, value):
         self._check(self.L.bk_set_option(self.ctx, self.OPTIONS[name], int(value)), "bk_set_option")

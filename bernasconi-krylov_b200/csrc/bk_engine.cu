@@ -97,6 +97,8 @@ struct bk_ctx {
   int e_recompute = 0;        // tile engine: 1 = E(s) recomputed from popcounts in A1, 0 = uint16 table
   int a1_wide = 0;            // per-pass schedule A1: 1 = 512 threads x 8 elements, 2 = warp-local (bits 0-8)
   int adj_a1 = 0;             // adjoint reverse sweep A1: 0 = 12-bit, 1 = warp-local (element bits 0-8)
+  uint32_t wait_polls = 0;    // persistent engine: polls of a dependency wait before it gives up (0 = default)
+  int64_t hold_step = -1;     // test hook: launch step whose dependency can never be met (-1 = off)
   std::map<int, uint16_t*> batch_E;  // E tables of batched runs, per n
   void* d_batch_state = nullptr;
   size_t batch_state_cap = 0;
@@ -766,6 +768,12 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   return BK_OK;
 }
 
+// Wait bounds and the test hook of a persistent launch, from the context's options.
+void program_limits(const bk_ctx* c, Program* P) {
+  P->poll_limit = c->wait_polls > 0 ? c->wait_polls : kWaitPolls * 4u;
+  P->hold_step = c->hold_step >= 0 ? (uint32_t)c->hold_step : 0xFFFFFFFFu;
+}
+
 // Steps [k0, k0 + n_steps) in one persistent launch, then `n_final`
 // measurement-only tasks (0 or all of them) for step k0 + n_steps; waits for the
 // launch and reports a bounded device wait that gave up.
@@ -788,6 +796,7 @@ int persist_launch(bk_ctx* c, PersistRun<R>& r, int k0, int n_steps, size_t n_fi
   P.next = r.next;
   P.err = r.err;
   P.abort = r.abort_w;
+  program_limits(c, &P);
   if (P.n_steps == 0 && P.n_final == 0) return BK_OK;
   size_t ev = 0;
   BK_TRY(ev_begin(c, "persist", &ev));
@@ -1165,6 +1174,7 @@ int evolve_batch_t(bk_ctx* c, const bk_batch_params* bp, const bk_batch_instance
   P.next = glob;
   P.err = reinterpret_cast<int*>(glob + 1);
   P.abort = reinterpret_cast<int*>(glob + 2);
+  program_limits(c, &P);
   const InstDesc<R>* dd = reinterpret_cast<const InstDesc<R>*>(base + o_desc);
 
   // the whole run: zero the states and counters, set the basis states, one persistent launch
@@ -1989,6 +1999,15 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
       if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "adjoint A1 %lld", (long long)value);
       c->adj_a1 = (int)value;
       return BK_OK;
+    case BK_OPT_WAIT_POLLS:
+      if (value != 0 && (value < 1000 || value > (int64_t)kWaitPolls * 4))
+        return fail(c, BK_ERR_INVALID, "wait polls %lld", (long long)value);
+      c->wait_polls = (uint32_t)value;
+      return BK_OK;
+    case BK_OPT_TEST_HOLD_STEP:
+      if (value < -1 || value > (int64_t)1 << 30) return fail(c, BK_ERR_INVALID, "hold step %lld", (long long)value);
+      c->hold_step = value;
+      return BK_OK;
     default:
       return fail(c, BK_ERR_INVALID, "unknown option %d", option);
   }
@@ -2003,6 +2022,8 @@ int bk_get_option(const bk_ctx* c, int option, int64_t* value) {
     case BK_OPT_E_SOURCE: *value = c->e_recompute; return BK_OK;
     case BK_OPT_A1_WIDE: *value = c->a1_wide; return BK_OK;
     case BK_OPT_ADJ_A1: *value = c->adj_a1; return BK_OK;
+    case BK_OPT_WAIT_POLLS: *value = c->wait_polls; return BK_OK;
+    case BK_OPT_TEST_HOLD_STEP: *value = c->hold_step; return BK_OK;
     default: return BK_ERR_INVALID;
   }
 }

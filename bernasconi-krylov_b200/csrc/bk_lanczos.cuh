@@ -128,6 +128,9 @@ __global__ void __launch_bounds__(kFsThreads, 2) fs_block_kernel(const double* _
     mbar_arrive_expect_tx(fb, 8u << kFsTileBits);
     bulk_load(smem_addr(ft), x + base, 8u << kFsTileBits, fb);
   }
+  // no thread may poll the barrier before thread 0 has initialised it (an SM's
+  // shared memory can still hold a completed barrier of an earlier CTA)
+  __syncthreads();
   double acc[kFsPer];
 #pragma unroll
   for (int k = 0; k < kFsPer; ++k) acc[k] = 0.0;
@@ -191,7 +194,8 @@ __global__ void __launch_bounds__(256) lz_orth_dot_kernel(double* __restrict__ w
 }
 
 // w -= alpha[ja] * v; partials[block] = sum of w^2
-__global__ void __launch_bounds__(256) lz_axpy_nrm_kernel(double* __restrict__ w, const double* __restrict__ v,
+// w and v may be the same vector (the start vector's norm): no __restrict__ on them
+__global__ void __launch_bounds__(256) lz_axpy_nrm_kernel(double* w, const double* v,
                                                           const double* __restrict__ alpha, int ja, uint64_t N,
                                                           double* __restrict__ partials) {
   __shared__ double red[8];
@@ -216,8 +220,9 @@ __global__ void lz_reduce_kernel(const double* __restrict__ partials, int count,
   if (threadIdx.x == 0) out[slot] = take_sqrt ? sqrt(s) : s;
 }
 
-// dst = src * (1 / norm[slot])
-__global__ void __launch_bounds__(256) lz_scale_kernel(double* __restrict__ dst, const double* __restrict__ src,
+// dst = src * (1 / norm[slot]); dst may equal src (in-place normalisation), so
+// neither is __restrict__
+__global__ void __launch_bounds__(256) lz_scale_kernel(double* dst, const double* src,
                                                        const double* __restrict__ norm, int slot, uint64_t N) {
   const double inv = 1.0 / norm[slot];
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x)

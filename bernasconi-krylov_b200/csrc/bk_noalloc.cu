@@ -8,6 +8,7 @@
 // and the output buffer, and the only scratch — the per-block partial sums and
 // the finishing ticket of the reduction — lives in the file-scope array below,
 // which every GPU that loads this library holds until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -26,6 +27,36 @@ static __device__ __align__(256) unsigned char bk_noalloc_scratch[kScratchBytes]
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned char* g_scratch_ptr[kMaxDevices] = {};  // device address of the array, per device
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // id of the context that address belongs to
+
+// Unique id of the calling thread's current context (cuCtxGetId never reuses an
+// id within a process), or 0 when the driver entry points are unavailable. A
+// cudaDeviceReset destroys the primary context and with it the array's
+// address; the next call sees a new id and resolves the address again.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+    looked_up = true;
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 template <class A>
 __global__ void __launch_bounds__(bk::kThreads) measure_noalloc_kernel(const A* __restrict__ psi, int n, int e0,
@@ -47,17 +78,26 @@ extern "C" int bk_measure_noalloc(int n, int precision, const void* d_state, int
                                   double* d_out, void* stream) {
   if (n < 1 || n > 30) return BK_ERR_TOO_LARGE;
   if (!d_state || !d_out || (precision != BK_C64 && precision != BK_C128)) return BK_ERR_INVALID;
+  // the kernel reads float2 / double2 amplitudes and writes doubles: a pointer
+  // off that alignment would fault on the device, so it is refused here
+  const uintptr_t state_align = precision == BK_C64 ? sizeof(float2) : sizeof(double2);
+  if (reinterpret_cast<uintptr_t>(d_state) % state_align != 0 || reinterpret_cast<uintptr_t>(d_out) % sizeof(double) != 0)
+    return BK_ERR_INVALID;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BK_ERR_CUDA;
   unsigned char* scratch = nullptr;
   {
-    // first call on this device: resolve the array's device address (the host
-    // symbol is only a stand-in); make this first call before any stream capture
+    // first call on this device (or in a new context of it): resolve the
+    // array's device address, the host symbol being only a stand-in; make this
+    // first call before any stream capture
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
+    const unsigned long long ctx_id = current_context_id();
+    if (!g_scratch_ptr[dev] || ctx_id != g_scratch_ctx[dev]) {
       void* p = nullptr;
       if (cudaGetSymbolAddress(&p, bk_noalloc_scratch) != cudaSuccess || !p) return BK_ERR_CUDA;
       g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+      // the lookup has made the device's context current if it was not yet
+      g_scratch_ctx[dev] = current_context_id();
     }
     scratch = g_scratch_ptr[dev];
   }

@@ -288,6 +288,11 @@ struct Program {
   unsigned int* next;               // work counter
   int* err;
   int* abort;
+  uint32_t poll_limit;              // bound on the polls of one dependency wait
+  // Test hook (0xFFFFFFFF = off): A1 / M tasks of this launch step wait for one
+  // completion more than can ever arrive, so their bounded wait runs out and
+  // the launch ends with DEV_TIMEOUT, as a lost producer would make it.
+  uint32_t hold_step;
 };
 
 __device__ __forceinline__ uint32_t ld_acquire(const unsigned int* p) {
@@ -619,10 +624,11 @@ __device__ __forceinline__ bool decode_task(const Program& P, uint32_t g, StageM
 
 // dependency of a task: counter and target (ctr == nullptr: none)
 template <class R>
-__device__ __forceinline__ const unsigned int* task_dep(const InstDesc<R>& D, const StageMeta& m, uint32_t& target) {
+__device__ __forceinline__ const unsigned int* task_dep(const InstDesc<R>& D, const StageMeta& m, uint32_t& target,
+                                                        const Program& P) {
   if (m.kind == TASK_A1 || m.kind == TASK_M) {
     if (m.step == 0) return nullptr;
-    target = (D.w3 > 0 ? D.n_s3 : D.n_s2) * m.step;
+    target = (D.w3 > 0 ? D.n_s3 : D.n_s2) * m.step + (m.step == P.hold_step ? 1u : 0u);
     return D.w3 > 0 ? D.s3_done : D.s2_done;
   }
   if (m.kind == TASK_S2) {
@@ -661,7 +667,7 @@ __device__ __forceinline__ void issue_task_load(const InstDesc<R>& D, const Stag
 __device__ __forceinline__ bool wait_counter(const unsigned int* ctr, uint32_t target, const Program& P) {
   uint32_t polls = 0;
   while (ld_acquire(ctr) < target) {
-    if (++polls > kWaitPolls * 4u) {
+    if (++polls > P.poll_limit) {
       raise_error(P, DEV_TIMEOUT);
       return false;
     }
@@ -715,7 +721,7 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
     } else {
       const InstDesc<R>& D = insts[cur.inst];
       uint32_t target = 0;
-      const unsigned int* ctr = task_dep(D, cur, target);
+      const unsigned int* ctr = task_dep(D, cur, target, P);
       if (ctr && !wait_counter(ctr, target, P)) cur.kind = TASK_END;
       if (cur.kind != TASK_END) {
         issue_task_load(D, cur, stage, fb);
@@ -736,7 +742,7 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
     if (tid == 0) {
       g_after = aborted(P.abort) ? 0xFFFFFFFFu : atomicAdd(P.next, 1u);
       if (nxt.kind != TASK_END) {
-        nctr = task_dep(insts[nxt.inst], nxt, ntarget);
+        nctr = task_dep(insts[nxt.inst], nxt, ntarget, P);
         if (nctr) nseen = ld_acquire(nctr);
       }
     }
@@ -812,7 +818,7 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
     if (tid == 0 && pending) {
       const InstDesc<R>& D2 = insts[cur.inst];
       uint32_t target = 0;
-      const unsigned int* ctr = task_dep(D2, cur, target);
+      const unsigned int* ctr = task_dep(D2, cur, target, P);
       if (wait_counter(ctr, target, P)) {
         issue_task_load(D2, cur, stage, fb);
         inflight = 1;

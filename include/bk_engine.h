@@ -281,14 +281,23 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       larger sizes run value 0);
  *   BK_OPT_ADJ_A1: bk_adjoint's reverse sweep, 1 = the warp-local A1 layout for
  *       both statevectors (element bits 0-8, strided passes from bit 9; up to 27
- *       element bits), 0 (default) = the 12-bit A1 of the forward geometry. */
+ *       element bits), 0 (default) = the 12-bit A1 of the forward geometry;
+ *   BK_OPT_WAIT_POLLS: persistent engine, polls of one dependency wait before
+ *       it gives up with BK_ERR_TIMEOUT (1000 .. 2^24; 0 = the default 2^24);
+ *   BK_OPT_TEST_HOLD_STEP: failure-path test hook, off (-1) by default: in the
+ *       persistent engine (BK_OPT_ENGINE_MODE 0), the A1 tasks of this step of a
+ *       launch wait for one completion more than can arrive, as if a producer
+ *       were lost; the bounded wait runs out, every CTA leaves, and bk_evolve
+ *       returns BK_ERR_TIMEOUT with the context still usable. */
 enum {
   BK_OPT_ENGINE_MODE = 0,
   BK_OPT_SLAB_LAG = 1,
   BK_OPT_SPLIT_W2 = 2,
   BK_OPT_E_SOURCE = 3,
   BK_OPT_A1_WIDE = 4,
-  BK_OPT_ADJ_A1 = 5
+  BK_OPT_ADJ_A1 = 5,
+  BK_OPT_WAIT_POLLS = 6,
+  BK_OPT_TEST_HOLD_STEP = 7
 };
 int bk_set_option(bk_ctx* ctx, int option, int64_t value);
 int bk_get_option(const bk_ctx* ctx, int option, int64_t* value);
@@ -358,10 +367,13 @@ int bk_sample(bk_ctx* ctx, const double* randnums, int64_t shots, uint64_t* out_
  * Allocates nothing: its scratch is a fixed 24.25 KiB array inside the library
  * (1024 block partial sums and a ticket), which every GPU that loads the
  * library holds until the process exits. Limit: 1 <= n <= 30, else
- * BK_ERR_TOO_LARGE. The first call on a device resolves the array's device
- * address; make that first call before any stream capture. All calls share the
- * array (it keeps the last call's contents; the ticket is cleared at the start
- * of every call), so calls that overlap on the GPU race: serialise them. */
+ * BK_ERR_TOO_LARGE; d_state must be aligned to its amplitude type (8 bytes for
+ * complex64, 16 for complex128) and d_out to 8 bytes, else BK_ERR_INVALID. The
+ * first call on a device resolves the array's device address, and so does the
+ * first call after the device's context was replaced (cudaDeviceReset); make
+ * that first call before any stream capture. All calls share the array (it
+ * keeps the last call's contents; the ticket is cleared at the start of every
+ * call), so calls that overlap on the GPU race: serialise them. */
 int bk_measure_noalloc(int n, int precision, const void* d_state, int64_t e0, uint64_t s0, double* d_out,
                        void* stream);
 

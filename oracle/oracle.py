@@ -126,6 +126,38 @@ def steepest_descent(n, start, max_evals=0, use_ref=False):
     return int(fs.value), int(fe.value), int(ev.value), int(st.value)
 
 
+def known_optimal_energy(n):
+    return int(lib().orc_known_optimal_energy(n))
+
+
+def select_trap(n, seed, n_descents, quantile, use_ref=None):
+    """Trap policy of the benchmark configurations (the lowest `quantile` of
+    `n_descents` seeded descents, global optima excluded, first minimum in
+    generation order at or below the threshold energy), restated on the
+    reference's descent: starts mt19937_64(seed) & mask
+    (classical.cuh:557-604), single-flip steepest descent (:625-712).
+    use_ref=None takes the reference's own compiled code when oracle/_ref was
+    built, else the oracle's restatement of it; both are bit-exact."""
+    if use_ref is None:
+        use_ref = ref_lib() is not None
+    if use_ref:
+        R = ref_lib()
+        starts = np.empty(n_descents, dtype=np.uint64)
+        R.ref_random_states(n, seed, n_descents, _ptr(starts, u64p))
+    else:
+        starts = random_states(n, seed, n_descents)
+    finals = [steepest_descent(n, int(x), 0, use_ref=use_ref)[:2] for x in starts]
+    opt = known_optimal_energy(n)
+    kept = sorted(e for _, e in finals if opt < 0 or e > opt)
+    if not kept:
+        raise ValueError(f"every descent at n = {n} reached a global optimum")
+    thr = kept[int(np.floor(quantile * (len(kept) - 1)))]
+    for bits, e in finals:
+        if (opt < 0 or e > opt) and e <= thr:
+            return bits, e
+    raise ValueError("no trap at or below the threshold")
+
+
 def uniform_randoms(seed, count):
     out = np.empty(count, dtype=np.float64)
     lib().orc_uniform_randoms(seed, count, _ptr(out, dp))

@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Regenerate the golden fixtures in this directory from the reference repository.
 
-Run in a container where the reference tree is mounted (default /root/reference);
+Run where the reference tree is checked out ($BK_REFERENCE_ROOT, default /root/reference);
 the GPU box never runs this. Every fixture is a small excerpt of a file the
 reference itself ships:
 
@@ -38,7 +38,7 @@ SERIES = {  # N -> list of (trap_rank, g or None for all three g)
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("BK_REFERENCE_ROOT", "/root/reference"))
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
     a = ap.parse_args()
     ex = os.path.join(a.ref, "data_raw/classical/exhaustive")

@@ -89,3 +89,11 @@ def test_select_trap_policy():
     first = next((b, e) for b, e in res if opt < e <= thr)
     assert (bits, e0) == first
     assert O.labs_energy(n, bits) == e0 and e0 > opt
+
+
+def test_oracle_trap_selection_equals_library():
+    # bench.py's reference arm selects its trap with the oracle (never the
+    # product library): both must give the same trap for every benchmark size
+    for n, seed, k, q in ((16, 42, 200, 0.05), (24, 42, 1000, 0.05), (28, 42, 4000, 0.01), (30, 42, 4000, 0.01)):
+        assert O.select_trap(n, seed, k, q) == tuple(bk.select_trap(n, seed, k, q))
+        assert O.select_trap(n, seed, k, q, use_ref=False) == tuple(bk.select_trap(n, seed, k, q))

@@ -13,7 +13,7 @@ import bk_b200 as bk
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "bernasconi-krylov_b200")
-REF = "/root/reference/src"
+REF = os.path.join(os.environ.get("BK_REFERENCE_ROOT", "/root/reference"), "src")
 
 
 def build_dropin_test(out):
