@@ -3,8 +3,11 @@ mixer is N cuStateVec calls per step, sampler.cuh:611-617).
 
 Knobs (engine options, include/bk_engine.h):
   engine_mode  0 = persistent dataflow kernel (every step in one launch, A1 tiles
-               handed to S2 through L2), 1 = one grid launch per pass;
-  slab_lag     persistent engine: slabs between a slab's A1 and S2 tasks;
+               handed to S2 through L2), 1 = one grid launch per pass, 2 = the
+               A1 pass as a grid launch and both strided passes in one
+               persistent launch (S3 re-reads S2's slabs from L2);
+  slab_lag     persistent engines: slabs between a slab's A1 and S2 tasks (mode
+               0), or between a slab's S2 and S3 tasks (mode 2);
   split_w2     qubits of the S2 pass (the rest go to S3), 0 = engine default;
   e_source     E(s) for the diagonal phase: 0 = uint16 table, 1 = recomputed
                from popcounts in the pass (no E traffic, more arithmetic);
@@ -69,6 +72,19 @@ def candidates(n, precision):
         d9 = default_w2(rest9)
         for w in [0] + [w for w in (d9 - 1, d9 + 1) if 3 <= w <= 9 and w <= rest9 and rest9 - w <= 9]:
             out.append(dict(engine_mode=1, slab_lag=3, split_w2=w, e_source=0, a1_wide=2))
+    # fused strided pass (mode 2: S2 and S3 in one launch, S3 reading S2's slabs
+    # from L2), for each A1 kernel and split that leaves a third pass to fuse
+    def fused(rest_bits, ws, wides):
+        for w in ws:
+            w2 = w if w else default_w2(rest_bits)
+            if rest_bits - w2 < 1:
+                continue
+            for wide in wides:
+                for lag in (1, 2, 3):
+                    out.append(dict(engine_mode=2, slab_lag=lag, split_w2=w, e_source=0, a1_wide=wide))
+    fused(rest, widths, (0, 1))
+    if 1 <= rest9 <= 18:
+        fused(rest9, [0] + [w for w in (d9 - 1, d9 + 1) if 3 <= w <= 9 and w <= rest9 and rest9 - w <= 9], (2,))
     # E recomputed in the pass, on the default split of both schedules
     out.append(dict(engine_mode=1, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))
     out.append(dict(engine_mode=0, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libbk_b200.so")
 SOURCES = ["csrc/bk_engine.cu", "csrc/bk_noalloc.cu"]
-HEADERS = ["csrc/bk_device.cuh", "csrc/bk_fused.cuh", "csrc/bk_aux.cuh", "csrc/bk_persist.cuh", "csrc/bk_adjoint.cuh", "csrc/bk_lanczos.cuh"]
+HEADERS = ["csrc/bk_device.cuh", "csrc/bk_fused.cuh", "csrc/bk_aux.cuh", "csrc/bk_persist.cuh", "csrc/bk_adjoint.cuh", "csrc/bk_lanczos.cuh", "csrc/bk_s23.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fopenmp", "-shared", "-ccbin", "/usr/bin/g++",

@@ -28,6 +28,7 @@
 #include "bk_fused.cuh"
 #include "bk_lanczos.cuh"
 #include "bk_persist.cuh"
+#include "bk_s23.cuh"
 
 using namespace bk;
 
@@ -592,6 +593,22 @@ struct PersistRun {
   int* abort_w = nullptr;
   uint32_t n_a1 = 0, n_s2 = 0, n_s3 = 0;
   typename PhaseV<R>::params phase{};  // device tables of the diagonal phase
+  // fused strided pass (engine mode 2): S2 / S3 tasks in slab order, counters
+  size_t o_tasks23 = 0, n_tasks23 = 0;
+  uint32_t slabs23 = 0, per_slab23 = 0;
+  unsigned int* ctr23 = nullptr;  // [slab_done: slabs23][next][ctas_done]
+};
+
+// Slab of a strided tile for the fused S2 + S3 pass: the element bits
+// [cpm, a1) (cpm = max(12 - w2, 12 - w3)) that neither tile covers. S2 tile ids
+// are mid | hi << (a1 - cp2) with mid = bits [cp2, a1); S3 tile ids are bits
+// [cp3, a1 + w2) (S3 reaches the top bit).
+struct SlabMap {
+  int cp2, cp3, cpm, bits;
+  uint32_t of_s2(uint32_t t, int mb2) const {
+    return ((t & ((1u << mb2) - 1u)) >> (cpm - cp2)) & ((1u << bits) - 1u);
+  }
+  uint32_t of_s3(uint32_t t) const { return (t >> (cpm - cp3)) & ((1u << bits) - 1u); }
 };
 
 // Width of the S2 pass for `rest` element bits above the A1 tile: the engine's
@@ -682,6 +699,34 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   const size_t o_hab = b.take(std::max<size_t>(hab.size(), 1) * sizeof(float2));
   const size_t o_ctr = b.take((slabs + 8) * sizeof(unsigned int));
   const size_t o_part = b.take(3 * (size_t)n_a1 * sizeof(double));
+  // fused strided pass: tasks in slab order (S3 of slab h after S2 of slab h + lag)
+  std::vector<unsigned long long> tasks23;
+  uint32_t slabs23 = 0, per_slab23 = 0;
+  if (grid_mode && c->engine_mode == 2 && w3 > 0) {
+    SlabMap sm{kElemBits - w2, kElemBits - w3, 0, 0};
+    sm.cpm = std::max(sm.cp2, sm.cp3);
+    sm.bits = std::max(0, a1_bits - sm.cpm);
+    slabs23 = 1u << sm.bits;
+    per_slab23 = n_s2 / slabs23;
+    std::vector<std::vector<uint32_t>> s2_of(slabs23), s3_of(slabs23);
+    for (uint32_t t = 0; t < n_s2; ++t) s2_of[sm.of_s2(t, a1_bits - sm.cp2)].push_back(t);
+    for (uint32_t t = 0; t < n_s3; ++t) s3_of[sm.of_s3(t)].push_back(t);
+    for (uint32_t v = 0; v < slabs23; ++v)
+      if (s2_of[v].size() != per_slab23 || s3_of[v].size() != n_s3 / slabs23)
+        return fail(c, BK_ERR_UNSUPPORTED, "fused strided pass: uneven slabs for n = %d", n);
+    const uint32_t lag23 = std::max<uint32_t>(1u, std::min<uint32_t>(slabs23, (uint32_t)c->slab_lag));
+    auto w23 = [](uint32_t kind, uint32_t slab, uint32_t tile) {
+      return ((unsigned long long)kind << 56) | ((unsigned long long)slab << 32) | tile;
+    };
+    for (uint32_t h = 0; h < slabs23 + lag23; ++h) {
+      if (h < slabs23)
+        for (uint32_t t : s2_of[h]) tasks23.push_back(w23(S23_S2, h, t));
+      if (h >= lag23)
+        for (uint32_t t : s3_of[h - lag23]) tasks23.push_back(w23(S23_S3, h - lag23, t));
+    }
+  }
+  const size_t o_tasks23 = b.take(std::max<size_t>(tasks23.size(), 1) * 8);
+  const size_t o_ctr23 = b.take((slabs23 + 4) * sizeof(unsigned int));
   BK_TRY(ensure_buffer(c, &c->d_persist, &c->persist_cap, b.off));
   char* base = static_cast<char*>(c->d_persist);
   CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(base + o_maps);
@@ -732,6 +777,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   D.e_recompute = c->e_recompute;
   D.a1_bits = a1_bits;
   D.map_a1s = d_maps + 4;
+  D.a1_evict_first = (grid_mode && c->engine_mode == 2) ? 1 : 0;
 
   cudaStream_t st = c->stream;
   BK_CUDA(c, cudaMemcpyAsync(d_maps, maps, sizeof(maps), cudaMemcpyHostToDevice, st));
@@ -745,6 +791,10 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   BK_CUDA(c, cudaMemcpyAsync(base + o_slot, S.slot.data(), S.slot.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   if (!hab.empty())
     BK_CUDA(c, cudaMemcpyAsync(base + o_hab, hab.data(), hab.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
+  if (!tasks23.empty()) {
+    BK_CUDA(c, cudaMemcpyAsync(base + o_tasks23, tasks23.data(), tasks23.size() * 8, cudaMemcpyHostToDevice, st));
+    BK_CUDA(c, cudaMemsetAsync(base + o_ctr23, 0, (slabs23 + 4) * sizeof(unsigned int), st));
+  }
   BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R, true>), PersistSmem::kBytes));
   run->base = base;
   run->o_desc = o_desc;
@@ -765,6 +815,11 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   run->n_s2 = n_s2;
   run->n_s3 = n_s3;
   run->phase = D.phase;
+  run->o_tasks23 = o_tasks23;
+  run->n_tasks23 = tasks23.size();
+  run->slabs23 = slabs23;
+  run->per_slab23 = per_slab23;
+  run->ctr23 = reinterpret_cast<unsigned int*>(base + o_ctr23);
   return BK_OK;
 }
 
@@ -816,7 +871,7 @@ template <class R>
 int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double angle_unit,
                    const std::vector<R>& tans, const std::vector<R>& scales) {
   PersistRun<R> run;
-  BK_TRY(persist_prepare<R>(c, p, S, angle_unit, tans, scales, &run, c->engine_mode == 1));
+  BK_TRY(persist_prepare<R>(c, p, S, angle_unit, tans, scales, &run, c->engine_mode != 0));
   const int n = p->n;
   cudaStream_t st = c->stream;
   unsigned int* ctr = run.ctr;
@@ -825,8 +880,23 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
   const uint32_t n_a1 = run.n_a1, n_s2 = run.n_s2, n_s3 = run.n_s3;
   const InstDesc<R> D = run.D;
 
-  if (c->engine_mode == 1) {
-    // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end
+  if (c->engine_mode == 1 || c->engine_mode == 2) {
+    // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end;
+    // mode 2 runs S2 + S3 as one fused launch (S3 reads S2's slabs from L2)
+    const bool fused23 = run.n_tasks23 > 0;
+    S23Program P23{};
+    if (fused23) {
+      BK_TRY(allow_smem(c, reinterpret_cast<const void*>(s23_kernel<R>), kS23Smem));
+      P23.tasks = reinterpret_cast<const unsigned long long*>(run.base + run.o_tasks23);
+      P23.n_tasks = (uint32_t)run.n_tasks23;
+      P23.per_slab = run.per_slab23;
+      P23.slab_done = run.ctr23;
+      P23.next = run.ctr23 + run.slabs23;
+      P23.ctas_done = run.ctr23 + run.slabs23 + 1;
+      P23.err = err;
+      P23.abort = reinterpret_cast<int*>(run.ctr23 + run.slabs23 + 2);
+      P23.poll_limit = c->wait_polls > 0 ? c->wait_polls : kWaitPolls * 4u;
+    }
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_pass_kernel<R>), PersistSmem::kBytes));
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_wide_kernel<R>), PersistSmem::kBytes));
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R>), kA1WarpSmem));
@@ -854,6 +924,14 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
         tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_A1, (uint32_t)k, err);
       BK_CUDA(c, cudaGetLastError());
       BK_TRY(ev_end(c, ev));
+      if (fused23) {
+        BK_TRY(ev_begin(c, "tile_s23", &ev));
+        P23.step = (uint32_t)k;
+        s23_kernel<R><<<c->num_sms, kS23Threads, kS23Smem, st>>>(D, P23);
+        BK_CUDA(c, cudaGetLastError());
+        BK_TRY(ev_end(c, ev));
+        continue;
+      }
       BK_TRY(ev_begin(c, "tile_s2", &ev));
       tile_pass_kernel<R><<<n_s2, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_S2, (uint32_t)k, err);
       BK_CUDA(c, cudaGetLastError());
@@ -1976,7 +2054,7 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
   if (!c) return BK_ERR_INVALID;
   switch (option) {
     case BK_OPT_ENGINE_MODE:
-      if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "engine mode %lld", (long long)value);
+      if (value < 0 || value > 2) return fail(c, BK_ERR_INVALID, "engine mode %lld", (long long)value);
       c->engine_mode = (int)value;
       return BK_OK;
     case BK_OPT_SLAB_LAG:

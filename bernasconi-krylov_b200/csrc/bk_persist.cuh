@@ -276,6 +276,7 @@ struct InstDesc {
   int e_recompute;               // 1: A1 / M recompute E(s) from popcounts instead of reading the E tile
   int a1_bits;                   // element bits the A1 pass butterflies (12; 9 for the warp-local A1)
   const CUtensorMap* map_a1s;    // warp-local A1: the A1 tile with the 128-byte TMA swizzle
+  int a1_evict_first;            // per-pass A1 stores: 1 = evict-first (its output is not re-read soon)
 };
 
 struct Program {
@@ -527,40 +528,54 @@ __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned c
     __syncthreads();
     stage_free();
     el_bflys<R, PL::A1_R3_REG, PL::A1_R3_ACT>(v, t);
-    el_gstore<R, PL::A1_R3_REG, kElemBits>(D.state, v, tile_base, b3, 0, policy_evict_last());
+    el_gstore<R, PL::A1_R3_REG, kElemBits>(D.state, v, tile_base, b3, 0,
+                                            D.a1_evict_first ? policy_evict_first() : policy_evict_last());
   }
   if (MEASURE_ONLY || slot >= 0)
     compute_reduce(acc, D.partials, D.ticket, D.results, MEASURE_ONLY ? D.slot[step] : slot, t_idx, D.n_a1, red,
                    last_flag);
 }
 
-// strided pass of width W on a staged tile (element bits [0, 12 - W) u [h0, h0 + W))
-template <class R, int W, class F>
+// Barrier over the threads that process one tile: the whole CTA (grid and
+// persistent kernels), or one 256-thread compute group of the fused strided
+// pass (named barrier `id`).
+struct CtaSync {
+  __device__ void sync() const { __syncthreads(); }
+};
+struct GroupSync {
+  uint32_t id;
+  __device__ void sync() const { asm volatile("bar.sync %0, 256;" ::"r"(id) : "memory"); }
+};
+
+// strided pass of width W on a staged tile (element bits [0, 12 - W) u [h0, h0 + W));
+// tid in [0, 256) is the thread's index in the tile's group, `sy` its barrier
+template <class R, int W, class Sync, class F>
 __device__ __forceinline__ void process_s(unsigned char* tile, unsigned char* state, uint32_t tile_base,
-                                          uint32_t h0, R t, F&& stage_free) {
+                                          uint32_t h0, R t, F&& stage_free, uint32_t tid, const Sync& sy,
+                                          uint64_t store_pol) {
   using PL = Plan<double>;
   using E = El<R>;
   constexpr int CP = kElemBits - W;
-  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t lane = tid & 31u, warp = tid >> 5;
   typename E::T v[16];
   constexpr uint32_t ACT_ALL = ((1u << W) - 1u) << CP;
   const uint32_t b1 = pdep(lane, PL::S_R1_LANE) | pdep(warp, PL::S_R1_WARP);
   el_load<R, PL::S_R1_REG, false>(tile, v, b1);
   if constexpr (W <= 4) {
-    __syncthreads();
+    sy.sync();
     stage_free();
   }
   el_bflys<R, PL::S_R1_REG, ACT_ALL>(v, t);
   if constexpr (W <= 4) {
-    el_gstore<R, PL::S_R1_REG, CP>(state, v, tile_base, b1, h0, policy_evict_first());
+    el_gstore<R, PL::S_R1_REG, CP>(state, v, tile_base, b1, h0, store_pol);
   } else {
     using R2 = StridedR2<double, W>;
     warp_sync();  // round-1 reads vs swizzled stores: same warp
     el_store_swz<R, PL::S_R1_REG>(tile, v, b1);
-    compute_sync();
+    sy.sync();
     const uint32_t b2 = pdep(lane, R2::LANE) | pdep(warp, R2::WARP);
     el_load<R, R2::REG, true>(tile, v, b2);
-    __syncthreads();
+    sy.sync();
     stage_free();
     el_bflys<R, R2::REG, R2::ACT>(v, t);
     if constexpr (R2::kShuffleLaneBit >= 0) {
@@ -570,24 +585,30 @@ __device__ __forceinline__ void process_s(unsigned char* tile, unsigned char* st
         E::bfly_partner(v[j], q, t);
       }
     }
-    el_gstore<R, R2::REG, CP>(state, v, tile_base, b2, h0, policy_evict_first());
+    el_gstore<R, R2::REG, CP>(state, v, tile_base, b2, h0, store_pol);
   }
 }
 
+template <class R, class Sync, class F>
+__device__ __forceinline__ void process_s_dispatch(int w, unsigned char* tile, unsigned char* state,
+                                                   uint32_t tile_base, uint32_t h0, R t, F&& f, uint32_t tid,
+                                                   const Sync& sy, uint64_t pol) {
+  switch (w) {
+    case 1: process_s<R, 1>(tile, state, tile_base, h0, t, f, tid, sy, pol); break;
+    case 2: process_s<R, 2>(tile, state, tile_base, h0, t, f, tid, sy, pol); break;
+    case 3: process_s<R, 3>(tile, state, tile_base, h0, t, f, tid, sy, pol); break;
+    case 4: process_s<R, 4>(tile, state, tile_base, h0, t, f, tid, sy, pol); break;
+    case 5: process_s<R, 5>(tile, state, tile_base, h0, t, f, tid, sy, pol); break;
+    case 6: process_s<R, 6>(tile, state, tile_base, h0, t, f, tid, sy, pol); break;
+    case 7: process_s<R, 7>(tile, state, tile_base, h0, t, f, tid, sy, pol); break;
+    case 8: process_s<R, 8>(tile, state, tile_base, h0, t, f, tid, sy, pol); break;
+    default: process_s<R, 9>(tile, state, tile_base, h0, t, f, tid, sy, pol); break;
+  }
+}
 template <class R, class F>
 __device__ __forceinline__ void process_s_dispatch(int w, unsigned char* tile, unsigned char* state,
                                                    uint32_t tile_base, uint32_t h0, R t, F&& f) {
-  switch (w) {
-    case 1: process_s<R, 1>(tile, state, tile_base, h0, t, f); break;
-    case 2: process_s<R, 2>(tile, state, tile_base, h0, t, f); break;
-    case 3: process_s<R, 3>(tile, state, tile_base, h0, t, f); break;
-    case 4: process_s<R, 4>(tile, state, tile_base, h0, t, f); break;
-    case 5: process_s<R, 5>(tile, state, tile_base, h0, t, f); break;
-    case 6: process_s<R, 6>(tile, state, tile_base, h0, t, f); break;
-    case 7: process_s<R, 7>(tile, state, tile_base, h0, t, f); break;
-    case 8: process_s<R, 8>(tile, state, tile_base, h0, t, f); break;
-    default: process_s<R, 9>(tile, state, tile_base, h0, t, f); break;
-  }
+  process_s_dispatch<R>(w, tile, state, tile_base, h0, t, f, threadIdx.x, CtaSync{}, policy_evict_first());
 }
 
 // ---------------------------------------------------------------------------
@@ -938,7 +959,7 @@ __global__ void __launch_bounds__(kA1WideThreads, 2)
   const uint32_t b4 = pdep(lane, PL::R4_LANE) | pdep(warp, PL::R4_WARP);
   el8_load<R, PL::R4_REG, true>(tile, v, b4);
   el8_bflys<R>(v, t);
-  const uint64_t pol = policy_evict_last();
+  const uint64_t pol = D.a1_evict_first ? policy_evict_first() : policy_evict_last();
 #pragma unroll
   for (int j = 0; j < 8; ++j) E::stg(D.state + 16ull * (tile_base | b4 | pdep((uint32_t)j, PL::R4_REG)), v[j], pol);
   if (slot >= 0)
@@ -1113,7 +1134,8 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
     const typename E::T q = E::shfl_xor(v[j], PL::kShuffleLanes);
     E::bfly_partner(v[j], q, t);
   }
-  el_gstore<R, PL::R2_REG, kElemBits>(D.state, v, tile_base, b2, 0, policy_evict_last());
+  el_gstore<R, PL::R2_REG, kElemBits>(D.state, v, tile_base, b2, 0,
+                                      D.a1_evict_first ? policy_evict_first() : policy_evict_last());
   if (slot >= 0) compute_reduce(acc, D.partials, D.ticket, D.results, slot, t_idx, D.n_a1, red, &last_flag);
 }
 

@@ -1,0 +1,199 @@
+// Fused strided pass (sm_100a): the S2 and S3 tile passes of one Trotter step in
+// ONE persistent launch, so that every element crosses HBM once per step in the
+// strided part instead of twice.
+//
+// Slabs. S2 tiles cover element bits [0, cp2) u [a1, a1 + w2), S3 tiles
+// [0, cp3) u [a1 + w2, np) (cp = 12 - w, a1 = the bits the A1 pass covers). The
+// bits [cpm, a1) with cpm = max(cp2, cp3) lie in neither tile: fixing them
+// gives a slab that both passes tile completely. An S3 tile of slab v needs
+// every S2 tile of slab v and nothing else, so with the tasks ordered
+//   S2(slab 0 .. L-1), then S3(slab v) before S2(slab v + L), ...
+// S3 re-reads a slab that S2 wrote a few slabs earlier, while it is still in
+// L2 (S2 stores evict-last; at N = 28 complex64 a slab is 16 MB). DRAM sees S2's
+// reads and S3's writes only.
+//
+// Warp roles, one CTA per SM:
+//   warp 0 (producer): claims tasks from a global counter in order, waits
+//     (bounded) for an S3 task's slab counter, and issues the TMA load into a
+//     ring of three 64 KB stages; a full barrier per stage carries the bytes,
+//     so two tiles are in flight from HBM while the third is computed.
+//   warps 1-8 (the compute group, 256 threads): the rounds of a tile run
+//     between the group's named barrier; after the tile's last shared-memory
+//     read the group frees the stage (empty barrier) and stores straight from
+//     registers. An S2 tile then releases its slab counter (one thread,
+//     red.release.gpu after the group barrier that orders all the group's
+//     stores before it).
+// Nine warps keep each SM sub-partition at three warps or fewer, so the tile
+// code keeps its registers (a second compute group would put five warps on
+// one sub-partition and cap every thread at 96 registers, spilling).
+// The producer never waits on a dependency before its earlier tasks are loaded,
+// and claims are global and in order, so the smallest unfinished task always
+// has its dependencies done, its stage free and its group idle: no deadlock.
+// Every wait is bounded; a timeout sets the error word and the abort flag that
+// every other wait polls, so the launch always ends.
+#pragma once
+#include "bk_persist.cuh"
+
+namespace bk {
+
+constexpr int kS23Stages = 3;
+constexpr int kS23Groups = 1;
+constexpr int kS23Threads = 32 + kS23Groups * kComputeThreads;  // 288
+constexpr int kS23Smem = kS23Stages * kStageTileBytes;          // 192 KB
+
+enum S23Kind : uint32_t { S23_S2 = 1, S23_S3 = 2, S23_END = 0xFF };
+
+// one launch = the strided part of one Trotter step
+struct S23Program {
+  const unsigned long long* tasks;  // kind << 56 | slab << 32 | tile, in claim order
+  uint32_t n_tasks;
+  uint32_t step;                    // Trotter step (tangent index, slab-counter epoch)
+  uint32_t per_slab;                // S2 tiles per slab
+  unsigned int* next;               // claim counter (reset by the last CTA to leave)
+  unsigned int* ctas_done;
+  unsigned int* slab_done;          // S2 completions per slab, cumulative over the steps of a call
+  int* err;
+  int* abort;
+  uint32_t poll_limit;
+};
+
+struct S23Task {
+  uint32_t kind, slab, tile;
+};
+
+__device__ __forceinline__ void red_release_add(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void s23_raise(const S23Program& P, int code) {
+  atomicCAS(P.err, 0, code);
+  atomicExch(P.abort, 1);
+}
+__device__ __forceinline__ bool s23_aborted(const S23Program& P) {
+  return *reinterpret_cast<const volatile int*>(P.abort) != 0;
+}
+// bounded wait on a stage barrier phase that also gives up on a global abort
+__device__ __forceinline__ bool s23_wait(uint32_t bar, uint32_t parity, const S23Program& P) {
+  for (uint32_t i = 0; i < kWaitPolls; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255u) == 255u && s23_aborted(P)) return false;
+  }
+  s23_raise(P, DEV_TIMEOUT);
+  return false;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kS23Threads, 1)
+    s23_kernel(const __grid_constant__ InstDesc<R> D, const __grid_constant__ S23Program P) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full_bar[kS23Stages];
+  __shared__ __align__(8) uint64_t empty_bar[kS23Stages];
+  __shared__ S23Task meta[kS23Stages];
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  if (tid == 0) {
+    for (int s = 0; s < kS23Stages; ++s) {
+      mbar_init(smem_addr(&full_bar[s]), 1);
+      mbar_init(smem_addr(&empty_bar[s]), 1);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  if (warp == 0) {
+    if (tid != 0) return;
+    // ---- producer ----
+    uint32_t armed[kS23Stages] = {0u, 0u, 0u};  // uses of each stage whose full phase was armed
+    uint32_t ends = 0;                           // END markers published (one per compute group)
+    for (uint32_t j = 0; ends < (uint32_t)kS23Groups; ++j) {
+      const uint32_t s = j % kS23Stages, u = j / kS23Stages;
+      if (u > 0 && !s23_wait(smem_addr(&empty_bar[s]), (u - 1u) & 1u, P)) break;
+      S23Task t{S23_END, 0u, 0u};
+      if (ends == 0u && !s23_aborted(P)) {
+        const uint32_t g = atomicAdd(P.next, 1u);
+        if (g < P.n_tasks) {
+          const unsigned long long w = P.tasks[g];
+          t.kind = (uint32_t)(w >> 56);
+          t.slab = (uint32_t)((w >> 32) & 0xFFFFFFu);
+          t.tile = (uint32_t)w;
+        }
+      }
+      if (t.kind == S23_S3) {
+        // every S2 tile of the slab, this step, must be in memory
+        const unsigned int* ctr = P.slab_done + t.slab;
+        const uint32_t target = P.per_slab * (P.step + 1u);
+        uint32_t polls = 0;
+        bool ok = true;
+        while (ld_acquire(ctr) < target) {
+          if (++polls > P.poll_limit) {
+            s23_raise(P, DEV_TIMEOUT);
+            ok = false;
+            break;
+          }
+          if ((polls & 63u) == 0u && s23_aborted(P)) {
+            ok = false;
+            break;
+          }
+          __nanosleep(64);
+        }
+        if (!ok) t.kind = S23_END;
+        else fence_proxy_async_global();  // the TMA reads what the counter released
+      }
+      meta[s] = t;
+      const uint32_t fb = smem_addr(&full_bar[s]);
+      if (t.kind == S23_END) {
+        ++ends;
+        mbar_arrive(fb);  // releases meta[s]; no bytes
+      } else {
+        StageMeta m;
+        m.kind = (t.kind == S23_S2) ? TASK_S2 : TASK_S3;
+        m.inst = 0;
+        m.tile = t.tile;
+        m.step = P.step;
+        issue_task_load(D, m, smem + (size_t)s * kStageTileBytes, fb);
+      }
+      armed[s] = u + 1u;
+    }
+    // loads still in flight land before the CTA leaves
+    for (int s = 0; s < kS23Stages; ++s)
+      if (armed[s] > 0u) mbar_wait_bounded(smem_addr(&full_bar[s]), (armed[s] - 1u) & 1u, P.err);
+    // the last CTA out resets the claim counter for the next launch
+    __threadfence();
+    if (atomicAdd(P.ctas_done, 1u) == gridDim.x - 1u) {
+      *P.next = 0u;
+      *P.ctas_done = 0u;
+    }
+    return;
+  }
+
+  // ---- compute group(s): group g takes the CTA's tasks g, g + kS23Groups, ... ----
+  const uint32_t grp = (warp - 1u) / 8u;
+  const uint32_t tg = tid - 32u - (uint32_t)kComputeThreads * grp;
+  const GroupSync sy{1u + grp};
+  const R t = D.tan[P.step];
+  for (uint32_t j = grp;; j += (uint32_t)kS23Groups) {
+    const uint32_t s = j % kS23Stages, u = j / kS23Stages;
+    if (!s23_wait(smem_addr(&full_bar[s]), u & 1u, P)) break;
+    const S23Task task = meta[s];
+    if (task.kind == S23_END) break;
+    unsigned char* stage = smem + (size_t)s * kStageTileBytes;
+    const uint32_t eb = smem_addr(&empty_bar[s]);
+    auto stage_free = [&]() {
+      if (tg == 0) mbar_arrive(eb);
+    };
+    const bool s2 = (task.kind == S23_S2);
+    const int w = s2 ? D.w2 : D.w3;
+    const int mb = s2 ? D.s2_mid_bits : D.s3_mid_bits;
+    const uint32_t h0 = s2 ? (uint32_t)D.a1_bits : (uint32_t)(D.a1_bits + D.w2);
+    const uint32_t cp = (uint32_t)(kElemBits - w);
+    const uint32_t mid = task.tile & ((1u << mb) - 1u), hi = task.tile >> mb;
+    const uint32_t tile_base = (mid << cp) | (hi << (h0 + (uint32_t)w));
+    // S2 output is re-read by S3 from L2; S3 output streams to DRAM
+    process_s_dispatch<R>(w, stage, D.state, tile_base, h0, t, stage_free, tg, sy,
+                          s2 ? policy_evict_last() : policy_evict_first());
+    if (s2) {
+      sy.sync();  // every store of the group's tile precedes the release below
+      if (tg == 0) red_release_add(P.slab_done + task.slab, 1u);
+    }
+  }
+}
+
+}  // namespace bk

@@ -266,7 +266,11 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
 
 /* Engine options (tuning knobs; the autotuner sets them from its cache):
  *   BK_OPT_ENGINE_MODE: 0 = persistent dataflow kernel (all steps in one launch,
- *       L2 hand-off between the A1 and S2 tasks), 1 = one grid launch per pass;
+ *       L2 hand-off between the A1 and S2 tasks), 1 = one grid launch per pass,
+ *       2 = a grid launch for the A1 pass and ONE persistent launch for both
+ *       strided passes (S3 re-reads each slab S2 wrote from L2, so the strided
+ *       part of a step crosses HBM once; sizes with a single strided pass run
+ *       as mode 1);
  *   BK_OPT_SLAB_LAG: persistent engine, slabs between A1 and S2 of a slab (>= 1);
  *   BK_OPT_SPLIT_W2: qubits of the S2 pass (1..9; the rest go to S3, at most 9),
  *       0 = the engine's default split; a width that does not fit a size is ignored;

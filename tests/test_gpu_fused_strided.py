@@ -1,0 +1,99 @@
+"""Engine mode 2: the A1 pass as a grid launch and both strided passes (S2, S3)
+as ONE persistent launch in which S3 re-reads, from L2, the slabs S2 has just
+written. Every element sees the same operations in the same order as with one
+launch per pass (mode 1), and the reductions are the same fixed-order sums, so
+the measured series must be bit-identical to mode 1 for every A1 kernel, S2
+width and slab lag; complex128 stays within 1e-10 of the oracle (the reference's
+step, src/sampling/sampler.cuh:604-618)."""
+import numpy as np
+import pytest
+
+import bk_b200 as bk
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    e = bk.Engine(0)
+    yield e
+    e.close()
+
+
+def _run(eng, n, precision, mode, a1, w2, lag=3, steps=12):
+    bits, e0 = bk.select_trap(n, 13, 200, 0.05)
+    g = np.random.default_rng(n + 7 * a1).uniform(0.25, 0.45, steps)
+    eng.set_option("engine_mode", mode)
+    eng.set_option("a1_wide", a1)
+    eng.set_option("split_w2", w2)
+    eng.set_option("slab_lag", lag)
+    try:
+        return eng.evolve(n, bits, g, 0.02, steps, measure=range(0, steps + 1, 3), e0=e0, precision=precision), \
+            (bits, e0, g)
+    finally:
+        eng.set_option("engine_mode", 0)
+        eng.set_option("a1_wide", 0)
+        eng.set_option("split_w2", 0)
+        eng.set_option("slab_lag", 3)
+
+
+# n, precision, A1 kernel (0: 256 threads, 1: 512 threads, 2: warp-local), S2 width (0: default)
+CASES = [
+    (22, bk.BK_C64, 0, 4), (24, bk.BK_C64, 0, 0), (24, bk.BK_C64, 1, 5), (26, bk.BK_C64, 1, 7),
+    (24, bk.BK_C64, 2, 0), (26, bk.BK_C64, 2, 8), (28, bk.BK_C64, 1, 7), (28, bk.BK_C64, 2, 0),
+    (21, bk.BK_C128, 0, 4), (23, bk.BK_C128, 1, 0), (25, bk.BK_C128, 2, 0),
+    (16, bk.BK_C64, 0, 0),  # a single strided pass: mode 2 runs it as mode 1
+]
+
+
+@pytest.mark.parametrize("n,precision,a1,w2", CASES)
+def test_fused_strided_equals_per_pass(eng, n, precision, a1, w2):
+    steps = 12 if n < 28 else 6
+    fused, _ = _run(eng, n, precision, 2, a1, w2, steps=steps)
+    per_pass, _ = _run(eng, n, precision, 1, a1, w2, steps=steps)
+    for a, b in zip(fused, per_pass):
+        assert np.array_equal(a, b), (n, precision, a1, w2)
+
+
+@pytest.mark.parametrize("lag", [1, 2, 8])
+def test_slab_lag_does_not_change_results(eng, lag):
+    ref, _ = _run(eng, 24, bk.BK_C64, 2, 1, 5, lag=3)
+    got, _ = _run(eng, 24, bk.BK_C64, 2, 1, 5, lag=lag)
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
+
+
+def test_fused_strided_matches_oracle_c128(eng):
+    n, steps = 21, 12
+    (p, d, nn), (bits, e0, g) = _run(eng, n, bk.BK_C128, 2, 0, 4, steps=steps)
+    po, do, _ = O.trotter_evolve(n, bits, e0, g, 0.02, steps, measure=range(0, steps + 1, 3))
+    assert np.max(np.abs(p - po)) <= 1e-10
+    assert np.max(np.abs(d - do)) <= 1e-10 * n
+    assert np.max(np.abs(nn - 1.0)) <= 1e-10
+
+
+def test_fused_strided_timeout_leaves_context_usable(eng):
+    """A bounded wait of the fused launch that runs out (the persistent engine's
+    hook does not reach mode 2, so the wait bound itself is made tiny while a
+    slab dependency is still open) must come back as an error or as a correct
+    result, never as a hang, and the context must keep working."""
+    n = 24
+    bits, e0 = bk.select_trap(n, 13, 200, 0.05)
+    eng.set_option("engine_mode", 2)
+    eng.set_option("wait_polls", 1000)
+    try:
+        try:
+            eng.evolve(n, bits, 0.35, 0.02, 4, measure=[4], e0=e0, precision=bk.BK_C64)
+        except bk.BkError as e:
+            assert e.status == bk._lib.BK_ERR_TIMEOUT
+    finally:
+        eng.set_option("wait_polls", 0)
+        eng.set_option("engine_mode", 0)
+    p, d, _ = eng.evolve(n, bits, 0.35, 0.02, 4, measure=[4], e0=e0, precision=bk.BK_C64)
+    eng.set_option("engine_mode", 2)
+    try:
+        p2, d2, _ = eng.evolve(n, bits, 0.35, 0.02, 4, measure=[4], e0=e0, precision=bk.BK_C64)
+    finally:
+        eng.set_option("engine_mode", 0)
+    assert abs(p2[0] - p[0]) <= 1e-6 and abs(d2[0] - d[0]) <= 1e-6 * n

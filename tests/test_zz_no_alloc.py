@@ -54,6 +54,44 @@ def test_noalloc_matches_engine_measurement(precision, n):
         assert abs(got[2] - nn[-1]) <= tol
 
 
+def test_noalloc_at_its_size_limit():
+    """n = 30, the entry point's largest size (complex64, 8 GiB statevector): the
+    same two-calls-in-a-row check against the engine's own measurement."""
+    import psutil
+    import torch
+    if psutil.virtual_memory().available < 48 * 2**30:
+        pytest.skip("needs ~40 GB of host memory for the exported n = 30 state")
+    n, steps = 30, 2
+    bits, e0 = bk.select_trap(n, 42, 100, 0.05)
+    with bk.Engine(0) as eng:
+        p, d, nn = eng.evolve(n, bits, 0.35, 0.05, steps, measure=[steps], e0=e0, precision=bk.BK_C64)
+        state = eng.export_state(n).astype(np.complex64)
+    dev = torch.device("cuda", 0)
+    d_state = torch.view_as_real(torch.from_numpy(state)).to(dev)
+    del state
+    d_out = torch.full((3,), float("nan"), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    L = _lib()
+    for _ in range(2):
+        d_out.fill_(float("nan"))
+        st = L.bk_measure_noalloc(n, bk.BK_C64, d_state.data_ptr(), e0, bits, d_out.data_ptr(), stream.cuda_stream)
+        assert st == 0
+        stream.synchronize()
+        got = d_out.cpu().numpy()
+        assert abs(got[0] - p[-1]) <= 1e-6
+        assert abs(got[1] - d[-1]) <= 1e-6 * n
+        assert abs(got[2] - nn[-1]) <= 1e-6
+
+
+def test_noalloc_rejects_misaligned_pointers():
+    L = _lib()
+    # refused on the host before any device work (a float2 / double2 read off
+    # its alignment would fault on the device)
+    assert L.bk_measure_noalloc(16, bk.BK_C64, ctypes.c_void_p(4096 + 4), -1, 0, ctypes.c_void_p(4096), None) == 1
+    assert L.bk_measure_noalloc(16, bk.BK_C128, ctypes.c_void_p(4096 + 8), -1, 0, ctypes.c_void_p(4096), None) == 1
+    assert L.bk_measure_noalloc(16, bk.BK_C64, ctypes.c_void_p(4096), -1, 0, ctypes.c_void_p(4096 + 4), None) == 1
+
+
 def test_noalloc_rejects_sizes_beyond_its_limit():
     L = _lib()
     # rejected on the host before any device work: n above the fixed limit of 30
