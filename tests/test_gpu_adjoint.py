@@ -174,3 +174,26 @@ def test_adjoint_warp_local_a1_c64_matches_oracle(eng, n):
     assert abs(val - oval) <= 1e-6
     assert np.max(np.abs(st["grad_steps"] - ograd)) <= 1e-4 * np.max(np.abs(ograd))
     assert st["max_drift"] <= 1e-4
+
+
+def test_adjoint_n28_full_schedule_checkpoints_sized_to_memory(eng):
+    """The large configuration's adjoint run in full: N = 28, 2000 steps (40
+    segments of 50, g_j ~ U[0.25, 0.45]), dt = 0.02, checkpoint interval left to
+    bk_adjoint's free-memory rule (128 steps, enlarged only when the checkpoints
+    would not fit in free HBM). complex64 against complex128 over the whole
+    run: objective within 1e-6, gradients within 1e-3 of the largest; the
+    objective equals bk_evolve's P_<(T) of the same schedule."""
+    n, T, nseg = 28, 2000, 40
+    bits, e0 = bk.select_trap(n, 42, 4000, 0.01)
+    gs = np.random.default_rng(2028).uniform(0.25, 0.45, nseg)
+    seg = O.segment_steps(T, nseg)
+    v64, g64, st64 = eng.adjoint(n, bits, gs, 0.02, T, e0=e0, precision=bk.BK_C64, checkpoint_every=0)
+    v128, g128, st128 = eng.adjoint(n, bits, gs, 0.02, T, e0=e0, precision=bk.BK_C128, checkpoint_every=0)
+    for st in (st64, st128):
+        assert st["checkpoint_every"] >= 128
+        assert st["n_checkpoints"] == (T - 1) // st["checkpoint_every"]
+    assert st64["max_drift"] <= 1e-4 and st128["max_drift"] <= 1e-11
+    assert abs(v64 - v128) <= 1e-6
+    assert np.max(np.abs(g64 - g128)) <= 1e-3 * np.max(np.abs(g128))
+    p, _, _ = eng.evolve(n, bits, gs[seg], 0.02, T, measure=[T], e0=e0, precision=bk.BK_C128)
+    assert abs(v128 - p[-1]) <= 1e-10
