@@ -54,13 +54,15 @@ def parse():
     ap.add_argument("--cpu-baseline-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
-    ap.add_argument("--engine-mode", type=int, default=None, help="0 persistent, 1 one launch per pass")
+    ap.add_argument("--engine-mode", type=int, default=None,
+                    help="0 persistent, 1 one launch per pass, 2 A1 launch + fused strided launch")
     ap.add_argument("--workload", choices=["large", "batched", "adjoint", "matvec"], default="large",
                     help="large: the N=28 headline; batched: 512 instances (64 traps x 8 g), N in {16,18,20,22}")
     ap.add_argument("--slab-lag", type=int, default=None)
     ap.add_argument("--split-w2", type=int, default=None, help="qubits of the S2 pass (0 = default split)")
-    ap.add_argument("--a1-kernel", type=int, default=None, choices=[0, 1, 2],
-                    help="per-pass A1 kernel: 0 = 256x16, 1 = 512x8, 2 = warp-local (element bits 0-8)")
+    ap.add_argument("--a1-kernel", type=int, default=None, choices=[0, 1, 2, 3],
+                    help="per-pass A1 kernel: 0 = 256x16, 1 = 512x8, 2 = warp-local (element bits 0-8), "
+                         "3 = warp-local over 32 KB half tiles")
     ap.add_argument("--no-tune", action="store_true", help="engine defaults instead of the autotuner's choice")
     ap.add_argument("--kernel-table-steps", type=int, default=3,
                     help="bench steps of the separate per-kernel timing pass (roofline)")

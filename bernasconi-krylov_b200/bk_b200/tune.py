@@ -14,7 +14,8 @@ Knobs (engine options, include/bk_engine.h):
   a1_wide      per-pass schedule, the A1 kernel: 0 = 256 threads x 16 elements
                (element bits 0-11), 1 = 512 x 8, 2 = warp-local (element bits
                0-8 inside each warp, no CTA barrier; the strided passes take
-               bits 9 and up; up to 27 element bits).
+               bits 9 and up; up to 27 element bits), 3 = warp-local with
+               4-warp CTAs over 32 KB half tiles (four CTAs per SM).
 For the batched engine the knob is the task-block lag between a statevector
 slab's A1 and S2 tasks.
 
@@ -71,7 +72,8 @@ def candidates(n, precision):
     if 1 <= rest9 <= 18:
         d9 = default_w2(rest9)
         for w in [0] + [w for w in (d9 - 1, d9 + 1) if 3 <= w <= 9 and w <= rest9 and rest9 - w <= 9]:
-            out.append(dict(engine_mode=1, slab_lag=3, split_w2=w, e_source=0, a1_wide=2))
+            for wide in (2, 3):
+                out.append(dict(engine_mode=1, slab_lag=3, split_w2=w, e_source=0, a1_wide=wide))
     # fused strided pass (mode 2: S2 and S3 in one launch, S3 reading S2's slabs
     # from L2), for each A1 kernel and split that leaves a third pass to fuse
     def fused(rest_bits, ws, wides):
@@ -84,7 +86,7 @@ def candidates(n, precision):
                     out.append(dict(engine_mode=2, slab_lag=lag, split_w2=w, e_source=0, a1_wide=wide))
     fused(rest, widths, (0, 1))
     if 1 <= rest9 <= 18:
-        fused(rest9, [0] + [w for w in (d9 - 1, d9 + 1) if 3 <= w <= 9 and w <= rest9 and rest9 - w <= 9], (2,))
+        fused(rest9, [0] + [w for w in (d9 - 1, d9 + 1) if 3 <= w <= 9 and w <= rest9 and rest9 - w <= 9], (2, 3))
     # E recomputed in the pass, on the default split of both schedules
     out.append(dict(engine_mode=1, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))
     out.append(dict(engine_mode=0, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))

@@ -297,14 +297,15 @@ int build_amp_map(bk_ctx* c, void* base, int n, int prec, int cp, int h0, int w,
 
 // A1 tiles (4096 16-byte elements, element bits [0, 12)) as 128-byte rows with the
 // 128-byte TMA swizzle, for the warp-local A1: dims (16, 256, 2, tiles) of
-// 8-byte units, box (16, 256, 2, 1); the tile index is coordinate 3.
-int build_a1_swizzled_map(bk_ctx* c, void* base, int np, TmaDesc* out) {
+// 8-byte units, box (16, 256, 2, 1); the tile index is coordinate 3. half: box
+// (16, 256, 1, 1), one 2048-element half tile per load (coordinates 2 and 3).
+int build_a1_swizzled_map(bk_ctx* c, void* base, int np, TmaDesc* out, bool half = false) {
   auto enc = encode_fn();
   if (!enc) return fail(c, BK_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable from the driver");
   const uint64_t total = (1ull << np) * 16;
   cuuint64_t gdim[5] = {16, 256, 2, 1ull << (np - kElemBits), 1};
   cuuint64_t gstride[4] = {128, 32768, 65536, total};
-  cuuint32_t box[5] = {16, 256, 2, 1, 1};
+  cuuint32_t box[5] = {16, 256, half ? 1u : 2u, 1, 1};
   cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   CUresult r = enc(&out->map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, base, gdim, gstride, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -632,7 +633,8 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   // the warp-local A1 (per-pass schedule) covers element bits 0-8; the strided
   // passes then take the remaining np - 9 <= 18 bits, the S2 width at least 3
   // (its tile keeps 12 - w2 <= 9 contiguous bits)
-  const bool a1_warp = grid_mode && c->a1_wide == 2 && np - kA1WarpBits <= 18;
+  const bool a1_warp = grid_mode && (c->a1_wide == 2 || c->a1_wide == 3) && np - kA1WarpBits <= 18;
+  const bool a1_half = a1_warp && c->a1_wide == 3;  // 4-warp CTAs over half tiles
   const int a1_bits = a1_warp ? kA1WarpBits : kElemBits;
   const int rest = np - a1_bits;
   int w2 = split_w2(c, rest);
@@ -642,12 +644,13 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   const int e_tile_bits = c64 ? 13 : 12;
 
   // tensor maps in element space (16-byte elements = two 8-byte TMA elements)
-  TmaDesc a1m, em, m2, m3, a1s;
+  TmaDesc a1m, em, m2, m3, a1s, eh;
   BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits, kElemBits, 0, &a1m));
   BK_TRY(build_e_map(c, c->d_E, n, e_tile_bits, &em));
   BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w2, a1_bits, w2, &m2));
   if (w3 > 0) BK_TRY(build_amp_map(c, c->d_state, np, BK_C128, kElemBits - w3, a1_bits + w2, w3, &m3));
-  if (a1_warp) BK_TRY(build_a1_swizzled_map(c, c->d_state, np, &a1s));
+  if (a1_warp) BK_TRY(build_a1_swizzled_map(c, c->d_state, np, &a1s, a1_half));
+  if (a1_half) BK_TRY(build_e_map(c, c->d_E, n, e_tile_bits - 1, &eh));
 
   // phase
   typename PhaseV<R>::params ph{};
@@ -689,7 +692,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
 
   // device buffer layout
   Bump b;
-  const size_t o_maps = b.take(5 * sizeof(CUtensorMap));
+  const size_t o_maps = b.take(6 * sizeof(CUtensorMap));
   const size_t o_desc = b.take(sizeof(InstDesc<R>));
   const size_t o_tasks = b.take(tasks.size() * 8);
   const size_t o_final = b.take(std::max<size_t>(final_tasks.size(), 1) * 8);
@@ -698,7 +701,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   const size_t o_slot = b.take(S.slot.size() * sizeof(int));
   const size_t o_hab = b.take(std::max<size_t>(hab.size(), 1) * sizeof(float2));
   const size_t o_ctr = b.take((slabs + 8) * sizeof(unsigned int));
-  const size_t o_part = b.take(3 * (size_t)n_a1 * sizeof(double));
+  const size_t o_part = b.take(3 * (size_t)n_a1 * (a1_half ? 2 : 1) * sizeof(double));
   // fused strided pass: tasks in slab order (S3 of slab h after S2 of slab h + lag)
   std::vector<unsigned long long> tasks23;
   uint32_t slabs23 = 0, per_slab23 = 0;
@@ -740,7 +743,8 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   int* err = reinterpret_cast<int*>(ctr + slabs + 4);
   int* abort_w = reinterpret_cast<int*>(ctr + slabs + 5);
 
-  CUtensorMap maps[5] = {a1m.map, em.map, m2.map, w3 > 0 ? m3.map : m2.map, a1_warp ? a1s.map : a1m.map};
+  CUtensorMap maps[6] = {a1m.map, em.map, m2.map, w3 > 0 ? m3.map : m2.map, a1_warp ? a1s.map : a1m.map,
+                         a1_half ? eh.map : em.map};
   InstDesc<R> D{};
   D.state = static_cast<unsigned char*>(c->d_state);
   D.map_a1 = d_maps + 0;
@@ -778,6 +782,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   D.a1_bits = a1_bits;
   D.map_a1s = d_maps + 4;
   D.a1_evict_first = (grid_mode && c->engine_mode == 2) ? 1 : 0;
+  D.map_e_half = d_maps + 5;
 
   cudaStream_t st = c->stream;
   BK_CUDA(c, cudaMemcpyAsync(d_maps, maps, sizeof(maps), cudaMemcpyHostToDevice, st));
@@ -899,7 +904,8 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
     }
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_pass_kernel<R>), PersistSmem::kBytes));
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_wide_kernel<R>), PersistSmem::kBytes));
-    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R>), kA1WarpSmem));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 8>), kA1WarpSmem));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 4>), HalfA1Smem::kBytes));
     using SampT = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
     BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
     for (int k = 0; k <= p->n_steps; ++k) {
@@ -916,8 +922,10 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
         break;
       }
       BK_TRY(ev_begin(c, "tile_a1", &ev));
-      if (D.a1_bits == kA1WarpBits)
-        tile_a1_warp_kernel<R><<<n_a1, kComputeThreads, kA1WarpSmem, st>>>(D, (uint32_t)k, err);
+      if (D.a1_bits == kA1WarpBits && c->a1_wide == 3)
+        tile_a1_warp_kernel<R, 4><<<2 * n_a1, 128, HalfA1Smem::kBytes, st>>>(D, (uint32_t)k, err);
+      else if (D.a1_bits == kA1WarpBits)
+        tile_a1_warp_kernel<R, 8><<<n_a1, kComputeThreads, kA1WarpSmem, st>>>(D, (uint32_t)k, err);
       else if (c->a1_wide == 1)
         tile_a1_wide_kernel<R><<<n_a1, kA1WideThreads, PersistSmem::kBytes, st>>>(D, (uint32_t)k, err);
       else
@@ -2070,7 +2078,7 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
       c->e_recompute = (int)value;
       return BK_OK;
     case BK_OPT_A1_WIDE:
-      if (value < 0 || value > 2) return fail(c, BK_ERR_INVALID, "A1 kernel %lld", (long long)value);
+      if (value < 0 || value > 3) return fail(c, BK_ERR_INVALID, "A1 kernel %lld", (long long)value);
       c->a1_wide = (int)value;
       return BK_OK;
     case BK_OPT_ADJ_A1:

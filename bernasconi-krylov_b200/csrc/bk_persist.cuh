@@ -277,6 +277,7 @@ struct InstDesc {
   int a1_bits;                   // element bits the A1 pass butterflies (12; 9 for the warp-local A1)
   const CUtensorMap* map_a1s;    // warp-local A1: the A1 tile with the 128-byte TMA swizzle
   int a1_evict_first;            // per-pass A1 stores: 1 = evict-first (its output is not re-read soon)
+  const CUtensorMap* map_e_half; // E of a half A1 tile (2^12 amplitude E values per box, complex64)
 };
 
 struct Program {
@@ -1056,34 +1057,61 @@ __device__ __forceinline__ void load_e8(const unsigned char* etile, uint32_t e, 
   }
 }
 
-template <class R>
-__global__ void __launch_bounds__(kComputeThreads, 2)
+// Shared-memory layout of the half-tile (4-warp) warp-local A1: a 32 KB tile,
+// then its E values (8 KB for complex64), the phase table and reduction scratch.
+struct HalfA1Smem {
+  static constexpr int kTileBytes = kStageTileBytes / 2;
+  static constexpr int kEOff = kTileBytes;
+  static constexpr int kPhaseOff = kEOff + kStageEBytes / 2;
+  static constexpr int kRedOff = kPhaseOff + 3328;
+  static constexpr int kBytes = kRedOff + 512 + 1024;  // + room to align the stage to 1024 bytes
+};
+
+// NW = 8: one CTA per 4096-element tile (64 KB); NW = 4: one CTA per half tile
+// (2048 elements, 32 KB; four CTAs per SM instead of two, so more independent
+// load -> compute -> store chains overlap on each SM). Each warp owns a 512-element
+// block either way: same arithmetic per element, bit-identical results.
+template <class R, int NW>
+__global__ void __launch_bounds__(NW * 32, 8 / NW * 2)
     tile_a1_warp_kernel(const __grid_constant__ InstDesc<R> D, uint32_t step, int* err) {
   using PL = PlanA1Warp;
   using E = El<R>;
+  static_assert(NW == 8 || NW == 4, "");
+  constexpr int kTB = kA1WarpBits + (NW == 8 ? 3 : 2);   // element bits of the CTA's tile
+  constexpr uint32_t kWarpMask = (NW == 8) ? PL::WARP : 0x600u;
+  constexpr uint32_t kTileBytes = 16u << kTB;
+  constexpr int kEOff = (NW == 8) ? kStageTileBytes : HalfA1Smem::kEOff;
+  constexpr int kPhaseOff = (NW == 8) ? PersistSmem::kPhaseOff : HalfA1Smem::kPhaseOff;
+  constexpr int kRedOff = (NW == 8) ? PersistSmem::kRedOff : HalfA1Smem::kRedOff;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar;
   __shared__ int last_flag;
   // the swizzled TMA destination must sit on a 1024-byte boundary
   unsigned char* smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
   unsigned char* tile = smem;
-  const unsigned char* etile = smem + kStageTileBytes;
-  unsigned char* phase_smem = smem + PersistSmem::kPhaseOff;
-  double* red = reinterpret_cast<double*>(smem + PersistSmem::kRedOff);
+  const unsigned char* etile = smem + kEOff;
+  unsigned char* phase_smem = smem + kPhaseOff;
+  double* red = reinterpret_cast<double*>(smem + kRedOff);
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t fb = smem_addr(&full_bar);
   const uint32_t t_idx = blockIdx.x;
-  const uint32_t tile_base = t_idx << kElemBits;
+  const uint32_t tile_base = t_idx << kTB;
   if (tid == 0) {
     mbar_init(fb, 1);
     fence_barrier_init();
     const bool e_tile = !D.e_recompute;
-    mbar_arrive_expect_tx(fb, (uint32_t)kStageTileBytes + (e_tile ? 4096u * 2u * (uint32_t)E::kAmps : 0u));
+    mbar_arrive_expect_tx(fb, kTileBytes + (e_tile ? (kTileBytes / 16u) * 2u * (uint32_t)E::kAmps : 0u));
     const uint64_t pol = policy_evict_first();
-    tma_load_5d_hint(smem_addr(tile), D.map_a1s, 0, 0, 0, (int)t_idx, 0, fb, pol);
-    if (e_tile) tma_load_5d_hint(smem_addr(tile + kStageTileBytes), D.map_e, 0, 0, (int)t_idx, 0, 0, fb, pol);
+    if constexpr (NW == 8) {
+      tma_load_5d_hint(smem_addr(tile), D.map_a1s, 0, 0, 0, (int)t_idx, 0, fb, pol);
+      if (e_tile) tma_load_5d_hint(smem_addr(tile + kEOff), D.map_e, 0, 0, (int)t_idx, 0, 0, fb, pol);
+    } else {
+      // half-tile maps: the A1 tile map with a box of one half, the E map with 2^12-amplitude tiles
+      tma_load_5d_hint(smem_addr(tile), D.map_a1s, 0, 0, (int)(t_idx & 1u), (int)(t_idx >> 1), 0, fb, pol);
+      if (e_tile) tma_load_5d_hint(smem_addr(tile + kEOff), D.map_e_half, 0, 0, (int)t_idx, 0, 0, fb, pol);
+    }
   }
-  PhaseV<R>::stage(D.phase, phase_smem, (int)tid, kComputeThreads);
+  PhaseV<R>::stage(D.phase, phase_smem, (int)tid, NW * 32);
   __syncthreads();
   const bool ok = mbar_wait_bounded(fb, 0, err);
   if (__syncthreads_or(!ok)) return;
@@ -1093,7 +1121,7 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
   MeasureAcc acc;
   // round 1 through the TMA swizzle (tile is 1024-byte aligned, so the swizzle
   // is a function of the tile offset)
-  const uint32_t b1 = pdep(lane, PL::R1_LANE) | pdep(warp, PL::WARP);
+  const uint32_t b1 = pdep(lane, PL::R1_LANE) | pdep(warp, kWarpMask);
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const uint32_t e = b1 | pdep((uint32_t)j, PL::R1_REG);
@@ -1126,7 +1154,7 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
   warp_sync();  // round-1 reads vs swizzled stores: same warp
   el_store_swz<R, PL::R1_REG>(tile, v, b1);
   warp_sync();  // rounds 1 and 2 share the warp bits
-  const uint32_t b2 = pdep(lane, PL::R2_LANE) | pdep(warp, PL::WARP);
+  const uint32_t b2 = pdep(lane, PL::R2_LANE) | pdep(warp, kWarpMask);
   el_load<R, PL::R2_REG, true>(tile, v, b2);
   el_bflys<R, PL::R2_REG, PL::R2_REG>(v, t);
 #pragma unroll
@@ -1136,7 +1164,8 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
   }
   el_gstore<R, PL::R2_REG, kElemBits>(D.state, v, tile_base, b2, 0,
                                       D.a1_evict_first ? policy_evict_first() : policy_evict_last());
-  if (slot >= 0) compute_reduce(acc, D.partials, D.ticket, D.results, slot, t_idx, D.n_a1, red, &last_flag);
+  if (slot >= 0)
+    compute_reduce<NW>(acc, D.partials, D.ticket, D.results, slot, t_idx, D.n_a1 * (8u / NW), red, &last_flag);
 }
 
 }  // namespace bk

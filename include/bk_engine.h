@@ -282,7 +282,8 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       warps per SM for the diagonal phase), 2 = warp-local: the A1 pass covers
  *       element bits 0-8, one warp per 512-element block with no CTA barrier,
  *       and the strided passes take bits 9 and up (sizes up to 27 element bits;
- *       larger sizes run value 0);
+ *       larger sizes run value 0), 3 = the same warp-local A1 with 4-warp CTAs
+ *       over half tiles (2048 elements, 32 KB; four CTAs per SM);
  *   BK_OPT_ADJ_A1: bk_adjoint's reverse sweep, 1 = the warp-local A1 layout for
  *       both statevectors (element bits 0-8, strided passes from bit 9; up to 27
  *       element bits), 0 (default) = the 12-bit A1 of the forward geometry;

@@ -97,3 +97,20 @@ def test_fused_strided_timeout_leaves_context_usable(eng):
     finally:
         eng.set_option("engine_mode", 0)
     assert abs(p2[0] - p[0]) <= 1e-6 and abs(d2[0] - d[0]) <= 1e-6 * n
+
+
+@pytest.mark.parametrize("n,precision,mode", [(24, bk.BK_C64, 1), (28, bk.BK_C64, 2), (23, bk.BK_C128, 2)])
+def test_half_tile_warp_local_a1_equals_full_tile(eng, n, precision, mode):
+    """BK_OPT_A1_WIDE = 3 runs the warp-local A1 with 4-warp CTAs over 32 KB half
+    tiles: every element gets the same arithmetic as with value 2, so the state
+    is bit-identical; the measurements sum twice as many per-tile partials, in
+    another fixed order, so they agree to FP64 rounding."""
+    steps = 12 if n < 28 else 6
+    out = {}
+    for a1 in (2, 3):
+        out[a1], _ = _run(eng, n, precision, mode, a1, 0, steps=steps)
+        out[a1] = out[a1] + (eng.export_state(n),)
+    (p2, d2, n2, s2), (p3, d3, n3, s3) = out[2], out[3]
+    assert np.array_equal(s2, s3)
+    assert np.max(np.abs(p2 - p3)) <= 1e-14 and np.max(np.abs(d2 - d3)) <= 1e-13 * n
+    assert np.max(np.abs(n2 - n3)) <= 1e-14

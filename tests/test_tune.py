@@ -12,16 +12,16 @@ def test_candidates_cover_modes_lags_and_valid_splits():
     assert {x["slab_lag"] for x in c if x["engine_mode"] == 0} == {1, 2, 3, 4, 6}
     assert {x["slab_lag"] for x in c if x["engine_mode"] == 2} == {1, 2, 3}
     assert {x["e_source"] for x in c} == {0, 1}
-    assert {x["a1_wide"] for x in c if x["engine_mode"] == 1} == {0, 1, 2}
-    assert {x["a1_wide"] for x in c if x["engine_mode"] == 2} == {0, 1, 2}
+    assert {x["a1_wide"] for x in c if x["engine_mode"] == 1} == {0, 1, 2, 3}
+    assert {x["a1_wide"] for x in c if x["engine_mode"] == 2} == {0, 1, 2, 3}
     for n, prec in ((30, bk.BK_C64), (30, bk.BK_C128), (22, bk.BK_C64), (14, bk.BK_C64)):
         np_ = n - 1 if prec == bk.BK_C64 else n
         for x in tune.candidates(n, prec):
             # the warp-local A1 leaves np - 9 bits to the strided passes, S2 at least 3
-            rest = np_ - (9 if x["a1_wide"] == 2 else tune.ELEM_BITS)
+            rest = np_ - (9 if x["a1_wide"] in (2, 3) else tune.ELEM_BITS)
             w = x["split_w2"] or tune.default_w2(rest)
             assert 1 <= w <= 9 and w <= rest and rest - w <= 9
-            assert x["a1_wide"] != 2 or (w >= 3 and x["engine_mode"] in (1, 2) and rest <= 18)
+            assert x["a1_wide"] not in (2, 3) or (w >= 3 and x["engine_mode"] in (1, 2) and rest <= 18)
             # the fused strided pass is only tried where a third pass is left to fuse
             assert x["engine_mode"] != 2 or rest - w >= 1
 
