@@ -23,7 +23,7 @@ def eng():
 
 def _run(eng, n, precision, mode, a1, w2, lag=3, steps=12):
     bits, e0 = bk.select_trap(n, 13, 200, 0.05)
-    g = np.random.default_rng(n + 7 * a1).uniform(0.25, 0.45, steps)
+    g = np.random.default_rng(n).uniform(0.25, 0.45, steps)
     eng.set_option("engine_mode", mode)
     eng.set_option("a1_wide", a1)
     eng.set_option("split_w2", w2)
