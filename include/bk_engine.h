@@ -148,7 +148,11 @@ typedef struct bk_evolve_params {
 } bk_evolve_params;
 
 /* Runs the whole schedule on the device and returns one row per flagged step:
- * p_less[m], d_h[m], norm[m] (host arrays of length sum(measure); norm may be NULL). */
+ * p_less[m], d_h[m], norm[m] (host arrays of length sum(measure); norm may be NULL).
+ * complex128 returns the reference's sums (sampler.cuh:149-195); complex64
+ * returns them divided by the measured |psi|^2 (the expectation values of the
+ * normalised state: FP32 rounding lets the norm wander ~1e-6 over thousands of
+ * steps), and norm[m] is always the raw |psi|^2. */
 int bk_evolve(bk_ctx* ctx, const bk_evolve_params* p, double* p_less, double* d_h, double* norm);
 
 /* ---- Batched evolution: many statevectors in one persistent launch ----
@@ -157,7 +161,7 @@ int bk_evolve(bk_ctx* ctx, const bk_evolve_params* p, double* p_less, double* d_
  * the measurement schedule. The tile tasks of all instances run in ONE
  * persistent kernel (launched through a captured CUDA graph when use_graph is
  * set), interleaved so that each statevector's A1 output is re-read from L2.
- * Outputs are row-major [instance][measurement]. */
+ * Outputs are row-major [instance][measurement], normalised like bk_evolve's. */
 typedef struct bk_batch_instance {
   int32_t n;           /* qubits: 14..30 (complex64) or 13..30 (complex128) */
   int32_t reserved;

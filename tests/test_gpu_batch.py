@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 import bk_b200 as bk
+from conftest import C64_DH_BAR, C64_DP_BAR
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -62,8 +63,8 @@ def test_batch_piecewise_schedules_c64(eng):
     pb, db, nb = eng.evolve_batch(inst, 0.02, steps, precision=bk.BK_C64)
     for i, d in enumerate(inst):
         po, do, _ = O.trotter_evolve(d["n"], d["s0"], d["e0"], d["g"], 0.02, steps)
-        assert np.max(np.abs(pb[i] - po)) <= 1e-6
-        assert np.max(np.abs(db[i] - do)) <= 1e-6 * d["n"]
+        assert np.max(np.abs(pb[i] - po)) <= C64_DP_BAR
+        assert np.max(np.abs(db[i] - do)) <= C64_DH_BAR
         assert np.max(np.abs(nb[i] - 1.0)) <= 1e-5
 
 

@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 import bk_b200 as bk
+from conftest import C64_DH_BAR, C64_DP_BAR
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -38,7 +39,7 @@ def test_norm_tolerance_reports_bk_err_norm():
         # the context is usable after the failure and its results are right
         po, do, _ = O.trotter_evolve(n, bits, e0, 0.35, 0.05, steps)
         p64, d64, _ = eng.evolve(n, bits, 0.35, 0.05, steps, e0=e0, precision=bk.BK_C64)
-        assert np.max(np.abs(p64 - po)) <= 1e-6
+        assert np.max(np.abs(p64 - po)) <= C64_DP_BAR
 
 
 @pytest.mark.parametrize("precision", [bk.BK_C64, bk.BK_C128])
@@ -58,9 +59,9 @@ def test_lost_dependency_reports_bk_err_timeout(precision):
         eng.set_option("wait_polls", 0)
         po, do, _ = O.trotter_evolve(n, bits, e0, 0.35, 0.05, steps)
         p, d, _ = eng.evolve(n, bits, 0.35, 0.05, steps, e0=e0, precision=precision)
-        tol = 1e-6 if precision == bk.BK_C64 else 1e-10
-        assert np.max(np.abs(p - po)) <= tol
-        assert np.max(np.abs(d - do)) <= tol * n
+        c64 = precision == bk.BK_C64
+        assert np.max(np.abs(p - po)) <= (C64_DP_BAR if c64 else 1e-10)
+        assert np.max(np.abs(d - do)) <= (C64_DH_BAR if c64 else 1e-10 * n)
 
 
 def test_option_ranges_are_checked():

@@ -9,8 +9,9 @@ itself pinned to the reference's own cuStateVec series at N = 24...30 by
 tests/test_gpu_parity.py::test_golden_series_c128.
 
 Bars (complex64 against complex128), written here:
-  * |dP_<| <= 1e-6 at every measured step;
-  * |d<d_H>| <= DH_BAR_C64 at every measured step;
+  * |dP_<| <= C64_DP_BAR (1e-6) at every measured step;
+  * |d<d_H>| <= C64_DH_BAR (3e-6) at every measured step (the reason is written
+    beside the constants in tests/conftest.py);
   * state infidelity 1 - |<psi_64|psi_128>|^2 <= 1e-8 at the end of the run.
 """
 import numpy as np
@@ -18,10 +19,9 @@ import pytest
 
 import bk_b200 as bk
 from bk_b200 import tune
+from conftest import C64_DH_BAR, C64_DP_BAR
 
 pytestmark = pytest.mark.gpu
-
-DH_BAR_C64 = 1e-6
 
 
 @pytest.fixture(scope="module")
@@ -57,8 +57,8 @@ def test_headline_n28_c64_tuned_against_c128(eng):
     (p128, d128, n128), _ = _evolve_tuned(eng, n, bk.BK_C128, bits, e0, 0.35, 0.02, steps, every)
     s128 = eng.export_state(n)
     assert len(p64) == steps // every + 1
-    assert np.max(np.abs(p64 - p128)) <= 1e-6
-    assert np.max(np.abs(d64 - d128)) <= DH_BAR_C64
+    assert np.max(np.abs(p64 - p128)) <= C64_DP_BAR
+    assert np.max(np.abs(d64 - d128)) <= C64_DH_BAR
     assert np.max(np.abs(n128 - 1.0)) <= 1e-10
     assert _infidelity(s64, s128) <= 1e-8
 
@@ -75,8 +75,8 @@ def test_large_n30_c64_tuned_against_c128_and_golden(eng, golden):
     (p64, d64, _), knobs = _evolve_tuned(eng, n, bk.BK_C64, bits, -1, s["g"], s["dt"], steps, every)
     assert knobs is not None
     (p128, d128, _), _ = _evolve_tuned(eng, n, bk.BK_C128, bits, -1, s["g"], s["dt"], steps, every)
-    assert np.max(np.abs(p64 - p128)) <= 1e-6
-    assert np.max(np.abs(d64 - d128)) <= DH_BAR_C64
+    assert np.max(np.abs(p64 - p128)) <= C64_DP_BAR
+    assert np.max(np.abs(d64 - d128)) <= C64_DH_BAR
     gp, gd = np.array(s["p_less"]), np.array(s["dh"])
-    assert np.all(np.abs(p64 - gp) <= 6e-7 * np.abs(gp) + 1e-6)
-    assert np.all(np.abs(d64 - gd) <= 5.01e-5 + DH_BAR_C64)
+    assert np.all(np.abs(p64 - gp) <= 6e-7 * np.abs(gp) + C64_DP_BAR)
+    assert np.all(np.abs(d64 - gd) <= 5.01e-5 + C64_DH_BAR)

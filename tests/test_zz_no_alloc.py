@@ -6,7 +6,9 @@ The caller (here: torch) owns the statevector and the 3-double output; the entry
 point's only scratch is a fixed array inside the library. Each case calls it twice
 in a row and checks both results against the engine's regular measurement
 (bk_evolve) of the same state, with the tolerances of the other parity tests:
-complex128 1e-10 (1e-10 * n for <d_H>), complex64 1e-6 (1e-6 * n). This file is
+complex128 1e-10 (1e-10 * n for <d_H>), complex64 1e-6 (3e-6 for <d_H>). bk_evolve
+returns complex64 sums divided by the state's norm, so they are multiplied back by
+the norm it reports before the comparison (this entry point returns raw sums). This file is
 collected last so that a run stopping at the first failure has run every other test.
 """
 import ctypes
@@ -42,15 +44,17 @@ def test_noalloc_matches_engine_measurement(precision, n):
     d_out = torch.full((3,), float("nan"), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
     L = _lib()
-    tol = 1e-10 if precision == bk.BK_C128 else 1e-6
+    c128 = precision == bk.BK_C128
+    tol, dtol = (1e-10, 1e-10 * n) if c128 else (1e-6, 3e-6)
+    raw = 1.0 if c128 else nn[-1]  # complex64 results come back normalised
     for _ in range(2):  # two calls in a row share the library's scratch array
         d_out.fill_(float("nan"))
         st = L.bk_measure_noalloc(n, precision, d_state.data_ptr(), e0, bits, d_out.data_ptr(), stream.cuda_stream)
         assert st == 0, bk._lib.load_library().bk_status_string(st)
         stream.synchronize()
         got = d_out.cpu().numpy()
-        assert abs(got[0] - p[-1]) <= tol
-        assert abs(got[1] - d[-1]) <= tol * n
+        assert abs(got[0] - p[-1] * raw) <= tol
+        assert abs(got[1] - d[-1] * raw) <= dtol
         assert abs(got[2] - nn[-1]) <= tol
 
 
@@ -78,8 +82,8 @@ def test_noalloc_at_its_size_limit():
         assert st == 0
         stream.synchronize()
         got = d_out.cpu().numpy()
-        assert abs(got[0] - p[-1]) <= 1e-6
-        assert abs(got[1] - d[-1]) <= 1e-6 * n
+        assert abs(got[0] - p[-1] * nn[-1]) <= 1e-6
+        assert abs(got[1] - d[-1] * nn[-1]) <= 3e-6
         assert abs(got[2] - nn[-1]) <= 1e-6
 
 
