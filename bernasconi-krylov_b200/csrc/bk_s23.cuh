@@ -22,7 +22,8 @@
 //     read the group frees the stage (empty barrier) and stores straight from
 //     registers. An S2 tile then releases its slab counter (one thread,
 //     red.release.gpu after the group barrier that orders all the group's
-//     stores before it).
+//     stores before it), deferred to the next tile's stage-free point so the
+//     group does not wait for its own stores to drain.
 // Nine warps keep each SM sub-partition at three warps or fewer, so the tile
 // code keeps its registers (a second compute group would put five warps on
 // one sub-partition and cap every thread at 96 registers, spilling).
@@ -169,15 +170,36 @@ __global__ void __launch_bounds__(kS23Threads, 1)
   const uint32_t tg = tid - 32u - (uint32_t)kComputeThreads * grp;
   const GroupSync sy{1u + grp};
   const R t = D.tan[P.step];
+  // The release of an S2 tile's slab counter is deferred to the group's next
+  // stage-free point: a release makes the releasing thread wait until every
+  // store it covers is performed, and by then the previous tile's stores have
+  // had a whole tile's compute to drain, while the current tile's are not yet
+  // issued. It is never held across a wait: if the next tile is not loaded yet
+  // (its load may depend on this very slab), the release goes out first.
+  // Only thread 0 of the group tracks it; the group barrier at the end of the
+  // S2 tile has made every thread's stores visible to it.
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  uint32_t pending = kNone;
   for (uint32_t j = grp;; j += (uint32_t)kS23Groups) {
     const uint32_t s = j % kS23Stages, u = j / kS23Stages;
-    if (!s23_wait(smem_addr(&full_bar[s]), u & 1u, P)) break;
+    const uint32_t fb = smem_addr(&full_bar[s]);
+    if (tg == 0 && pending != kNone && !mbar_try_wait(fb, u & 1u)) {
+      red_release_add(P.slab_done + pending, 1u);
+      pending = kNone;
+    }
+    if (!s23_wait(fb, u & 1u, P)) break;
     const S23Task task = meta[s];
     if (task.kind == S23_END) break;
     unsigned char* stage = smem + (size_t)s * kStageTileBytes;
     const uint32_t eb = smem_addr(&empty_bar[s]);
     auto stage_free = [&]() {
-      if (tg == 0) mbar_arrive(eb);
+      if (tg == 0) {
+        mbar_arrive(eb);
+        if (pending != kNone) {
+          red_release_add(P.slab_done + pending, 1u);
+          pending = kNone;
+        }
+      }
     };
     const bool s2 = (task.kind == S23_S2);
     const int w = s2 ? D.w2 : D.w3;
@@ -190,10 +212,11 @@ __global__ void __launch_bounds__(kS23Threads, 1)
     process_s_dispatch<R>(w, stage, D.state, tile_base, h0, t, stage_free, tg, sy,
                           s2 ? policy_evict_last() : policy_evict_first());
     if (s2) {
-      sy.sync();  // every store of the group's tile precedes the release below
-      if (tg == 0) red_release_add(P.slab_done + task.slab, 1u);
+      sy.sync();  // every store of the group's tile precedes the (deferred) release
+      if (tg == 0) pending = task.slab;
     }
   }
+  if (tg == 0 && pending != kNone) red_release_add(P.slab_done + pending, 1u);
 }
 
 }  // namespace bk
