@@ -77,8 +77,13 @@ def test_adjoint_value_is_the_forward_measurement(eng, precision):
     bits, e0, gs, seg = _case(n, 5, T, 9)
     val, _, st = eng.adjoint(n, bits, gs, 0.02, T, e0=e0, precision=precision, checkpoint_every=16)
     p, d, nn = eng.evolve(n, bits, gs[seg], 0.02, T, measure=[T], e0=e0, precision=precision)
-    assert val == p[0]
     assert st["norm"] == nn[0]
+    if precision == bk.BK_C128:
+        assert val == p[0]
+    else:
+        # bk_evolve returns complex64 sums divided by the norm; the adjoint's
+        # objective is the raw sum whose gradient it returns
+        assert val == pytest.approx(p[0] * nn[0], rel=1e-14, abs=0.0)
 
 
 def test_adjoint_segment_gradients_match_finite_differences_n22(eng):
