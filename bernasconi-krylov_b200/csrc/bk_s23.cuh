@@ -13,7 +13,8 @@
 // reads and S3's writes only.
 //
 // Warp roles, one CTA per SM:
-//   warp 0 (producer): claims tasks from a global counter in order, waits
+//   warp 0 (producer): claims tasks from a global counter in order (batches
+//     of kS23Batch consecutive tasks, processed in order), waits
 //     (bounded) for an S3 task's slab counter, and issues the TMA load into a
 //     ring of three 64 KB stages; a full barrier per stage carries the bytes,
 //     so two tiles are in flight from HBM while the third is computed.
@@ -41,6 +42,8 @@ constexpr int kS23Stages = 3;
 constexpr int kS23Groups = 1;
 constexpr int kS23Threads = 32 + kS23Groups * kComputeThreads;  // 288
 constexpr int kS23Smem = kS23Stages * kStageTileBytes;          // 192 KB
+constexpr int kS23Batch = 8;                                     // tasks per claim
+static_assert(kS23Stages == 3, "the producer tracks three stages by name");
 
 enum S23Kind : uint32_t { S23_S2 = 1, S23_S3 = 2, S23_END = 0xFF };
 
@@ -102,60 +105,86 @@ __global__ void __launch_bounds__(kS23Threads, 1)
   if (warp == 0) {
     if (tid != 0) return;
     // ---- producer ----
-    uint32_t armed[kS23Stages] = {0u, 0u, 0u};  // uses of each stage whose full phase was armed
-    uint32_t ends = 0;                           // END markers published (one per compute group)
-    for (uint32_t j = 0; ends < (uint32_t)kS23Groups; ++j) {
-      const uint32_t s = j % kS23Stages, u = j / kS23Stages;
-      if (u > 0 && !s23_wait(smem_addr(&empty_bar[s]), (u - 1u) & 1u, P)) break;
-      S23Task t{S23_END, 0u, 0u};
-      if (ends == 0u && !s23_aborted(P)) {
-        const uint32_t g = atomicAdd(P.next, 1u);
-        if (g < P.n_tasks) {
-          const unsigned long long w = P.tasks[g];
-          t.kind = (uint32_t)(w >> 56);
-          t.slab = (uint32_t)((w >> 32) & 0xFFFFFFu);
-          t.tile = (uint32_t)w;
+    // Claims come in batches of kS23Batch consecutive tasks, the next batch's
+    // claim in flight while this one is loaded; a batch's task words are read
+    // together (one memory latency per batch); a slab counter seen complete is
+    // not read again for the same slab. Per task the producer then only waits
+    // for a free stage and issues the TMA.
+    __shared__ unsigned long long words[kS23Batch];
+    uint32_t armed0 = 0u, armed1 = 0u, armed2 = 0u;  // uses of each stage whose full phase was armed
+    uint32_t ends = 0;                                // END markers published (one per compute group)
+    uint32_t ok_slab = 0xFFFFFFFFu;                   // slab whose S2 tiles are known complete this step
+    const uint32_t target = P.per_slab * (P.step + 1u);
+    uint32_t base = s23_aborted(P) ? P.n_tasks : atomicAdd(P.next, (uint32_t)kS23Batch);
+    bool stop = false;
+    for (uint32_t j = 0; ends < (uint32_t)kS23Groups && !stop;) {
+      // this batch's task words, and the next batch's claim (used one batch later)
+      unsigned long long wl[kS23Batch];
+#pragma unroll
+      for (int k = 0; k < kS23Batch; ++k)  // all loads in flight together
+        wl[k] = (base + (uint32_t)k < P.n_tasks) ? P.tasks[base + k] : ((unsigned long long)S23_END << 56);
+#pragma unroll
+      for (int k = 0; k < kS23Batch; ++k) words[k] = wl[k];
+      const uint32_t next_base = (base >= P.n_tasks || s23_aborted(P)) ? P.n_tasks
+                                                                       : atomicAdd(P.next, (uint32_t)kS23Batch);
+      for (uint32_t k = 0; k < (uint32_t)kS23Batch && ends < (uint32_t)kS23Groups; ++k, ++j) {
+        const uint32_t s = j % kS23Stages, u = j / kS23Stages;
+        if (u > 0 && !s23_wait(smem_addr(&empty_bar[s]), (u - 1u) & 1u, P)) {
+          stop = true;
+          break;
         }
-      }
-      if (t.kind == S23_S3) {
-        // every S2 tile of the slab, this step, must be in memory
-        const unsigned int* ctr = P.slab_done + t.slab;
-        const uint32_t target = P.per_slab * (P.step + 1u);
-        uint32_t polls = 0;
-        bool ok = true;
-        while (ld_acquire(ctr) < target) {
-          if (++polls > P.poll_limit) {
-            s23_raise(P, DEV_TIMEOUT);
-            ok = false;
-            break;
+        const unsigned long long w = words[k];
+        S23Task t;
+        t.kind = (ends > 0u || s23_aborted(P)) ? (uint32_t)S23_END : (uint32_t)(w >> 56);
+        t.slab = (uint32_t)((w >> 32) & 0xFFFFFFu);
+        t.tile = (uint32_t)w;
+        if (t.kind == S23_S3 && t.slab != ok_slab) {
+          // every S2 tile of the slab, this step, must be in memory
+          const unsigned int* ctr = P.slab_done + t.slab;
+          uint32_t polls = 0;
+          bool ok = true;
+          while (ld_acquire(ctr) < target) {
+            if (++polls > P.poll_limit) {
+              s23_raise(P, DEV_TIMEOUT);
+              ok = false;
+              break;
+            }
+            if ((polls & 63u) == 0u && s23_aborted(P)) {
+              ok = false;
+              break;
+            }
+            __nanosleep(64);
           }
-          if ((polls & 63u) == 0u && s23_aborted(P)) {
-            ok = false;
-            break;
+          if (!ok) {
+            t.kind = S23_END;
+          } else {
+            fence_proxy_async_global();  // the TMA reads what the counter released
+            ok_slab = t.slab;
           }
-          __nanosleep(64);
         }
-        if (!ok) t.kind = S23_END;
-        else fence_proxy_async_global();  // the TMA reads what the counter released
+        meta[s] = t;
+        const uint32_t fb = smem_addr(&full_bar[s]);
+        if (t.kind == S23_END) {
+          ++ends;
+          mbar_arrive(fb);  // releases meta[s]; no bytes
+        } else {
+          StageMeta m;
+          m.kind = (t.kind == S23_S2) ? TASK_S2 : TASK_S3;
+          m.inst = 0;
+          m.tile = t.tile;
+          m.step = P.step;
+          issue_task_load(D, m, smem + (size_t)s * kStageTileBytes, fb);
+        }
+        if (s == 0) armed0 = u + 1u;
+        else if (s == 1) armed1 = u + 1u;
+        else armed2 = u + 1u;
       }
-      meta[s] = t;
-      const uint32_t fb = smem_addr(&full_bar[s]);
-      if (t.kind == S23_END) {
-        ++ends;
-        mbar_arrive(fb);  // releases meta[s]; no bytes
-      } else {
-        StageMeta m;
-        m.kind = (t.kind == S23_S2) ? TASK_S2 : TASK_S3;
-        m.inst = 0;
-        m.tile = t.tile;
-        m.step = P.step;
-        issue_task_load(D, m, smem + (size_t)s * kStageTileBytes, fb);
-      }
-      armed[s] = u + 1u;
+      base = next_base;
     }
     // loads still in flight land before the CTA leaves
-    for (int s = 0; s < kS23Stages; ++s)
-      if (armed[s] > 0u) mbar_wait_bounded(smem_addr(&full_bar[s]), (armed[s] - 1u) & 1u, P.err);
+    if (armed0 > 0u) mbar_wait_bounded(smem_addr(&full_bar[0]), (armed0 - 1u) & 1u, P.err);
+    if (armed1 > 0u) mbar_wait_bounded(smem_addr(&full_bar[1]), (armed1 - 1u) & 1u, P.err);
+    if (armed2 > 0u) mbar_wait_bounded(smem_addr(&full_bar[2]), (armed2 - 1u) & 1u, P.err);
     // the last CTA out resets the claim counter for the next launch
     __threadfence();
     if (atomicAdd(P.ctas_done, 1u) == gridDim.x - 1u) {
