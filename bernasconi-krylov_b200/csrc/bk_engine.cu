@@ -99,6 +99,7 @@ struct bk_ctx {
   int a1_wide = 0;            // per-pass schedule A1: 1 = 512 threads x 8 elements, 2 = warp-local (bits 0-8)
   int adj_a1 = 0;             // adjoint reverse sweep A1: 0 = 12-bit, 1 = warp-local (element bits 0-8)
   uint32_t wait_polls = 0;    // persistent engine: polls of a dependency wait before it gives up (0 = default)
+  uint64_t s23_checked = 0;   // fused strided pass geometry (np, a1, w2, lag) whose closed form was checked
   int64_t hold_step = -1;     // test hook: launch step whose dependency can never be met (-1 = off)
   std::map<int, uint16_t*> batch_E;  // E tables of batched runs, per n
   void* d_batch_state = nullptr;
@@ -595,9 +596,10 @@ struct PersistRun {
   uint32_t n_a1 = 0, n_s2 = 0, n_s3 = 0;
   typename PhaseV<R>::params phase{};  // device tables of the diagonal phase
   // fused strided pass (engine mode 2): S2 / S3 tasks in slab order, counters
-  size_t o_tasks23 = 0, n_tasks23 = 0;
-  uint32_t slabs23 = 0, per_slab23 = 0;
-  unsigned int* ctr23 = nullptr;  // [slab_done: slabs23][next][ctas_done]
+  size_t n_tasks23 = 0;
+  uint32_t slabs23 = 0;
+  S23Program prog23{};            // the task order's closed form (counters set at launch)
+  unsigned int* ctr23 = nullptr;  // [slab_done: slabs23][next][ctas_done][abort]
 };
 
 // Slab of a strided tile for the fused S2 + S3 pass: the element bits
@@ -705,30 +707,55 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   // fused strided pass: tasks in slab order (S3 of slab h after S2 of slab h + lag)
   std::vector<unsigned long long> tasks23;
   uint32_t slabs23 = 0, per_slab23 = 0;
+  S23Program prog23{};
   if (grid_mode && c->engine_mode == 2 && w3 > 0) {
     SlabMap sm{kElemBits - w2, kElemBits - w3, 0, 0};
     sm.cpm = std::max(sm.cp2, sm.cp3);
     sm.bits = std::max(0, a1_bits - sm.cpm);
     slabs23 = 1u << sm.bits;
     per_slab23 = n_s2 / slabs23;
-    std::vector<std::vector<uint32_t>> s2_of(slabs23), s3_of(slabs23);
-    for (uint32_t t = 0; t < n_s2; ++t) s2_of[sm.of_s2(t, a1_bits - sm.cp2)].push_back(t);
-    for (uint32_t t = 0; t < n_s3; ++t) s3_of[sm.of_s3(t)].push_back(t);
-    for (uint32_t v = 0; v < slabs23; ++v)
-      if (s2_of[v].size() != per_slab23 || s3_of[v].size() != n_s3 / slabs23)
-        return fail(c, BK_ERR_UNSUPPORTED, "fused strided pass: uneven slabs for n = %d", n);
     const uint32_t lag23 = std::max<uint32_t>(1u, std::min<uint32_t>(slabs23, (uint32_t)c->slab_lag));
-    auto w23 = [](uint32_t kind, uint32_t slab, uint32_t tile) {
-      return ((unsigned long long)kind << 56) | ((unsigned long long)slab << 32) | tile;
-    };
-    for (uint32_t h = 0; h < slabs23 + lag23; ++h) {
-      if (h < slabs23)
-        for (uint32_t t : s2_of[h]) tasks23.push_back(w23(S23_S2, h, t));
-      if (h >= lag23)
-        for (uint32_t t : s3_of[h - lag23]) tasks23.push_back(w23(S23_S3, h - lag23, t));
+    const uint64_t key = ((uint64_t)np << 48) | ((uint64_t)a1_bits << 40) | ((uint64_t)w2 << 32) | lag23;
+    int lb = 0;
+    while ((1u << lb) < per_slab23) ++lb;
+    prog23.slabs = slabs23;
+    prog23.lag = lag23;
+    prog23.lb = (uint32_t)lb;
+    prog23.x = (uint32_t)(sm.cpm - sm.cp2);
+    prog23.y = (uint32_t)(sm.cpm - sm.cp3);
+    prog23.mb2 = (uint32_t)(a1_bits - sm.cp2);
+    prog23.bits = (uint32_t)sm.bits;
+    prog23.n_tasks = 2u * n_s2;
+    if ((1u << lb) != per_slab23 || n_s3 != n_s2)
+      return fail(c, BK_ERR_UNSUPPORTED, "fused strided pass: slab size not a power of two for n = %d", n);
+    // the kernel decodes its task order in closed form; the first run of a
+    // geometry checks it against the order built here tile by tile
+    if (c->s23_checked != key) {
+      std::vector<std::vector<uint32_t>> s2_of(slabs23), s3_of(slabs23);
+      for (uint32_t t = 0; t < n_s2; ++t) s2_of[sm.of_s2(t, a1_bits - sm.cp2)].push_back(t);
+      for (uint32_t t = 0; t < n_s3; ++t) s3_of[sm.of_s3(t)].push_back(t);
+      for (uint32_t v = 0; v < slabs23; ++v)
+        if (s2_of[v].size() != per_slab23 || s3_of[v].size() != n_s3 / slabs23)
+          return fail(c, BK_ERR_UNSUPPORTED, "fused strided pass: uneven slabs for n = %d", n);
+      auto w23 = [](uint32_t kind, uint32_t slab, uint32_t tile) {
+        return ((unsigned long long)kind << 56) | ((unsigned long long)slab << 32) | tile;
+      };
+      for (uint32_t h = 0; h < slabs23 + lag23; ++h) {
+        if (h < slabs23)
+          for (uint32_t t : s2_of[h]) tasks23.push_back(w23(S23_S2, h, t));
+        if (h >= lag23)
+          for (uint32_t t : s3_of[h - lag23]) tasks23.push_back(w23(S23_S3, h - lag23, t));
+      }
+      if (tasks23.size() != prog23.n_tasks)
+        return fail(c, BK_ERR_UNSUPPORTED, "fused strided pass: %zu tasks for n = %d", tasks23.size(), n);
+      for (uint32_t g = 0; g < prog23.n_tasks; ++g) {
+        const S23Task t = s23_decode(prog23, g);
+        if (w23(t.kind, t.slab, t.tile) != tasks23[g])
+          return fail(c, BK_ERR_UNSUPPORTED, "fused strided pass: task order mismatch at %u (n = %d)", g, n);
+      }
+      c->s23_checked = key;
     }
   }
-  const size_t o_tasks23 = b.take(std::max<size_t>(tasks23.size(), 1) * 8);
   const size_t o_ctr23 = b.take((slabs23 + 4) * sizeof(unsigned int));
   BK_TRY(ensure_buffer(c, &c->d_persist, &c->persist_cap, b.off));
   char* base = static_cast<char*>(c->d_persist);
@@ -796,10 +823,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   BK_CUDA(c, cudaMemcpyAsync(base + o_slot, S.slot.data(), S.slot.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   if (!hab.empty())
     BK_CUDA(c, cudaMemcpyAsync(base + o_hab, hab.data(), hab.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
-  if (!tasks23.empty()) {
-    BK_CUDA(c, cudaMemcpyAsync(base + o_tasks23, tasks23.data(), tasks23.size() * 8, cudaMemcpyHostToDevice, st));
-    BK_CUDA(c, cudaMemsetAsync(base + o_ctr23, 0, (slabs23 + 4) * sizeof(unsigned int), st));
-  }
+  if (prog23.n_tasks > 0) BK_CUDA(c, cudaMemsetAsync(base + o_ctr23, 0, (slabs23 + 4) * sizeof(unsigned int), st));
   BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R, true>), PersistSmem::kBytes));
   run->base = base;
   run->o_desc = o_desc;
@@ -820,10 +844,9 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   run->n_s2 = n_s2;
   run->n_s3 = n_s3;
   run->phase = D.phase;
-  run->o_tasks23 = o_tasks23;
-  run->n_tasks23 = tasks23.size();
+  run->n_tasks23 = prog23.n_tasks;
   run->slabs23 = slabs23;
-  run->per_slab23 = per_slab23;
+  run->prog23 = prog23;
   run->ctr23 = reinterpret_cast<unsigned int*>(base + o_ctr23);
   return BK_OK;
 }
@@ -889,12 +912,9 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
     // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end;
     // mode 2 runs S2 + S3 as one fused launch (S3 reads S2's slabs from L2)
     const bool fused23 = run.n_tasks23 > 0;
-    S23Program P23{};
+    S23Program P23 = run.prog23;
     if (fused23) {
       BK_TRY(allow_smem(c, reinterpret_cast<const void*>(s23_kernel<R>), kS23Smem));
-      P23.tasks = reinterpret_cast<const unsigned long long*>(run.base + run.o_tasks23);
-      P23.n_tasks = (uint32_t)run.n_tasks23;
-      P23.per_slab = run.per_slab23;
       P23.slab_done = run.ctr23;
       P23.next = run.ctr23 + run.slabs23;
       P23.ctas_done = run.ctr23 + run.slabs23 + 1;

@@ -13,8 +13,8 @@
 // reads and S3's writes only.
 //
 // Warp roles, one CTA per SM:
-//   warp 0 (producer): claims tasks from a global counter in order (batches
-//     of kS23Batch consecutive tasks, processed in order), waits
+//   warp 0 (producer): claims tasks one at a time from a global counter in
+//     order (the next claim already in flight), waits
 //     (bounded) for an S3 task's slab counter, and issues the TMA load into a
 //     ring of three 64 KB stages; a full barrier per stage carries the bytes,
 //     so two tiles are in flight from HBM while the third is computed.
@@ -42,17 +42,19 @@ constexpr int kS23Stages = 3;
 constexpr int kS23Groups = 1;
 constexpr int kS23Threads = 32 + kS23Groups * kComputeThreads;  // 288
 constexpr int kS23Smem = kS23Stages * kStageTileBytes;          // 192 KB
-constexpr int kS23Batch = 8;                                     // tasks per claim
 static_assert(kS23Stages == 3, "the producer tracks three stages by name");
 
 enum S23Kind : uint32_t { S23_S2 = 1, S23_S3 = 2, S23_END = 0xFF };
 
 // one launch = the strided part of one Trotter step
 struct S23Program {
-  const unsigned long long* tasks;  // kind << 56 | slab << 32 | tile, in claim order
+  // task order (claim index g -> task): for h = 0 .. slabs + lag - 1, the S2
+  // tiles of slab h (h < slabs), then the S3 tiles of slab h - lag (h >= lag),
+  // 2^lb tiles each in increasing tile id; decoded in closed form (s23_decode)
+  uint32_t slabs, lag, lb;          // slab count, S2 -> S3 lag in slabs, log2 tiles per slab and pass
+  uint32_t x, y, mb2, bits;         // cpm - cp2, cpm - cp3, S2 mid bits, slab bits
   uint32_t n_tasks;
   uint32_t step;                    // Trotter step (tangent index, slab-counter epoch)
-  uint32_t per_slab;                // S2 tiles per slab
   unsigned int* next;               // claim counter (reset by the last CTA to leave)
   unsigned int* ctas_done;
   unsigned int* slab_done;          // S2 completions per slab, cumulative over the steps of a call
@@ -64,6 +66,39 @@ struct S23Program {
 struct S23Task {
   uint32_t kind, slab, tile;
 };
+
+// Task g of the launch's claim order (g < n_tasks). S2 tiles of slab v are
+// mid | hi << mb2 with mid = v << x | low; S3 tiles are low | v << y | up << (y + bits).
+__host__ __device__ inline S23Task s23_decode(const S23Program& P, uint32_t g) {
+  const uint32_t B = 1u << P.lb;
+  uint32_t kind, v, i;
+  if (g < P.lag * B) {
+    kind = S23_S2;
+    v = g >> P.lb;
+    i = g & (B - 1u);
+  } else {
+    const uint32_t g1 = g - P.lag * B;
+    if (g1 < 2u * B * (P.slabs - P.lag)) {
+      const uint32_t pr = g1 >> (P.lb + 1u), r = g1 & (2u * B - 1u);
+      kind = r < B ? S23_S2 : S23_S3;
+      v = r < B ? P.lag + pr : pr;
+      i = r & (B - 1u);
+    } else {
+      const uint32_t g2 = g1 - 2u * B * (P.slabs - P.lag);
+      kind = S23_S3;
+      v = P.slabs - P.lag + (g2 >> P.lb);
+      i = g2 & (B - 1u);
+    }
+  }
+  S23Task t;
+  t.kind = kind;
+  t.slab = v;
+  if (kind == S23_S2)
+    t.tile = (v << P.x) | (i & ((1u << P.x) - 1u)) | ((i >> P.x) << P.mb2);
+  else
+    t.tile = (i & ((1u << P.y) - 1u)) | (v << P.y) | ((i >> P.y) << (P.y + P.bits));
+  return t;
+}
 
 __device__ __forceinline__ void red_release_add(unsigned int* p, unsigned int v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
@@ -105,81 +140,63 @@ __global__ void __launch_bounds__(kS23Threads, 1)
   if (warp == 0) {
     if (tid != 0) return;
     // ---- producer ----
-    // Claims come in batches of kS23Batch consecutive tasks, the next batch's
-    // claim in flight while this one is loaded; a batch's task words are read
-    // together (one memory latency per batch); a slab counter seen complete is
-    // not read again for the same slab. Per task the producer then only waits
-    // for a free stage and issues the TMA.
-    __shared__ unsigned long long words[kS23Batch];
+    // One task claimed at a time (the GPU's window of tasks in progress stays
+    // a few per SM, so S3 tiles find their slab finished and in L2), with the
+    // next claim's atomic in flight while this task waits for its stage; the
+    // task itself is decoded from its index (no memory read), and a slab
+    // counter seen complete is not read again for the same slab.
     uint32_t armed0 = 0u, armed1 = 0u, armed2 = 0u;  // uses of each stage whose full phase was armed
     uint32_t ends = 0;                                // END markers published (one per compute group)
     uint32_t ok_slab = 0xFFFFFFFFu;                   // slab whose S2 tiles are known complete this step
-    const uint32_t target = P.per_slab * (P.step + 1u);
-    uint32_t base = s23_aborted(P) ? P.n_tasks : atomicAdd(P.next, (uint32_t)kS23Batch);
-    bool stop = false;
-    for (uint32_t j = 0; ends < (uint32_t)kS23Groups && !stop;) {
-      // this batch's task words, and the next batch's claim (used one batch later)
-      unsigned long long wl[kS23Batch];
-#pragma unroll
-      for (int k = 0; k < kS23Batch; ++k)  // all loads in flight together
-        wl[k] = (base + (uint32_t)k < P.n_tasks) ? P.tasks[base + k] : ((unsigned long long)S23_END << 56);
-#pragma unroll
-      for (int k = 0; k < kS23Batch; ++k) words[k] = wl[k];
-      const uint32_t next_base = (base >= P.n_tasks || s23_aborted(P)) ? P.n_tasks
-                                                                       : atomicAdd(P.next, (uint32_t)kS23Batch);
-      for (uint32_t k = 0; k < (uint32_t)kS23Batch && ends < (uint32_t)kS23Groups; ++k, ++j) {
-        const uint32_t s = j % kS23Stages, u = j / kS23Stages;
-        if (u > 0 && !s23_wait(smem_addr(&empty_bar[s]), (u - 1u) & 1u, P)) {
-          stop = true;
-          break;
-        }
-        const unsigned long long w = words[k];
-        S23Task t;
-        t.kind = (ends > 0u || s23_aborted(P)) ? (uint32_t)S23_END : (uint32_t)(w >> 56);
-        t.slab = (uint32_t)((w >> 32) & 0xFFFFFFu);
-        t.tile = (uint32_t)w;
-        if (t.kind == S23_S3 && t.slab != ok_slab) {
-          // every S2 tile of the slab, this step, must be in memory
-          const unsigned int* ctr = P.slab_done + t.slab;
-          uint32_t polls = 0;
-          bool ok = true;
-          while (ld_acquire(ctr) < target) {
-            if (++polls > P.poll_limit) {
-              s23_raise(P, DEV_TIMEOUT);
-              ok = false;
-              break;
-            }
-            if ((polls & 63u) == 0u && s23_aborted(P)) {
-              ok = false;
-              break;
-            }
-            __nanosleep(64);
+    const uint32_t target = (1u << P.lb) * (P.step + 1u);
+    uint32_t g_next = s23_aborted(P) ? P.n_tasks : atomicAdd(P.next, 1u);
+    for (uint32_t j = 0; ends < (uint32_t)kS23Groups; ++j) {
+      const uint32_t s = j % kS23Stages, u = j / kS23Stages;
+      const uint32_t g = g_next;
+      if (ends == 0u) g_next = (g >= P.n_tasks || s23_aborted(P)) ? P.n_tasks : atomicAdd(P.next, 1u);
+      if (u > 0 && !s23_wait(smem_addr(&empty_bar[s]), (u - 1u) & 1u, P)) break;
+      S23Task t{S23_END, 0u, 0u};
+      if (ends == 0u && g < P.n_tasks && !s23_aborted(P)) t = s23_decode(P, g);
+      if (t.kind == S23_S3 && t.slab != ok_slab) {
+        // every S2 tile of the slab, this step, must be in memory
+        const unsigned int* ctr = P.slab_done + t.slab;
+        uint32_t polls = 0;
+        bool ok = true;
+        while (ld_acquire(ctr) < target) {
+          if (++polls > P.poll_limit) {
+            s23_raise(P, DEV_TIMEOUT);
+            ok = false;
+            break;
           }
-          if (!ok) {
-            t.kind = S23_END;
-          } else {
-            fence_proxy_async_global();  // the TMA reads what the counter released
-            ok_slab = t.slab;
+          if ((polls & 63u) == 0u && s23_aborted(P)) {
+            ok = false;
+            break;
           }
+          __nanosleep(64);
         }
-        meta[s] = t;
-        const uint32_t fb = smem_addr(&full_bar[s]);
-        if (t.kind == S23_END) {
-          ++ends;
-          mbar_arrive(fb);  // releases meta[s]; no bytes
+        if (!ok) {
+          t.kind = S23_END;
         } else {
-          StageMeta m;
-          m.kind = (t.kind == S23_S2) ? TASK_S2 : TASK_S3;
-          m.inst = 0;
-          m.tile = t.tile;
-          m.step = P.step;
-          issue_task_load(D, m, smem + (size_t)s * kStageTileBytes, fb);
+          fence_proxy_async_global();  // the TMA reads what the counter released
+          ok_slab = t.slab;
         }
-        if (s == 0) armed0 = u + 1u;
-        else if (s == 1) armed1 = u + 1u;
-        else armed2 = u + 1u;
       }
-      base = next_base;
+      meta[s] = t;
+      const uint32_t fb = smem_addr(&full_bar[s]);
+      if (t.kind == S23_END) {
+        ++ends;
+        mbar_arrive(fb);  // releases meta[s]; no bytes
+      } else {
+        StageMeta m;
+        m.kind = (t.kind == S23_S2) ? TASK_S2 : TASK_S3;
+        m.inst = 0;
+        m.tile = t.tile;
+        m.step = P.step;
+        issue_task_load(D, m, smem + (size_t)s * kStageTileBytes, fb);
+      }
+      if (s == 0) armed0 = u + 1u;
+      else if (s == 1) armed1 = u + 1u;
+      else armed2 = u + 1u;
     }
     // loads still in flight land before the CTA leaves
     if (armed0 > 0u) mbar_wait_bounded(smem_addr(&full_bar[0]), (armed0 - 1u) & 1u, P.err);
