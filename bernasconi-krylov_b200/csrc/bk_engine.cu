@@ -704,7 +704,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   const size_t o_hab = b.take(std::max<size_t>(hab.size(), 1) * sizeof(float2));
   const size_t o_ctr = b.take((slabs + 8) * sizeof(unsigned int));
   const size_t o_part = b.take(3 * (size_t)n_a1 * (a1_half ? 2 : 1) * sizeof(double));
-  // fused strided pass: tasks in slab order (S3 of slab h after S2 of slab h + lag)
+  // fused strided pass: tasks in slab order (S2 of slab h after S3 of slab h + lag)
   std::vector<unsigned long long> tasks23;
   uint32_t slabs23 = 0, per_slab23 = 0;
   S23Program prog23{};
@@ -740,11 +740,11 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
       auto w23 = [](uint32_t kind, uint32_t slab, uint32_t tile) {
         return ((unsigned long long)kind << 56) | ((unsigned long long)slab << 32) | tile;
       };
-      for (uint32_t h = 0; h < slabs23 + lag23; ++h) {
+      for (uint32_t h = 0; h < slabs23 + lag23; ++h) {  // S3 of a slab first, its S2 lag slabs later
         if (h < slabs23)
-          for (uint32_t t : s2_of[h]) tasks23.push_back(w23(S23_S2, h, t));
+          for (uint32_t t : s3_of[h]) tasks23.push_back(w23(S23_S3, h, t));
         if (h >= lag23)
-          for (uint32_t t : s3_of[h - lag23]) tasks23.push_back(w23(S23_S3, h - lag23, t));
+          for (uint32_t t : s2_of[h - lag23]) tasks23.push_back(w23(S23_S2, h - lag23, t));
       }
       if (tasks23.size() != prog23.n_tasks)
         return fail(c, BK_ERR_UNSUPPORTED, "fused strided pass: %zu tasks for n = %d", tasks23.size(), n);

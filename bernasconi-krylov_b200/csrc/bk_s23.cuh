@@ -5,12 +5,17 @@
 // Slabs. S2 tiles cover element bits [0, cp2) u [a1, a1 + w2), S3 tiles
 // [0, cp3) u [a1 + w2, np) (cp = 12 - w, a1 = the bits the A1 pass covers). The
 // bits [cpm, a1) with cpm = max(cp2, cp3) lie in neither tile: fixing them
-// gives a slab that both passes tile completely. An S3 tile of slab v needs
-// every S2 tile of slab v and nothing else, so with the tasks ordered
-//   S2(slab 0 .. L-1), then S3(slab v) before S2(slab v + L), ...
-// S3 re-reads a slab that S2 wrote a few slabs earlier, while it is still in
-// L2 (S2 stores evict-last; at N = 28 complex64 a slab is 16 MB). DRAM sees S2's
-// reads and S3's writes only.
+// gives a slab that both passes tile completely. The Rx gates of different
+// qubits commute, so either pass may go first; the high-bit pass S3 goes first
+// because its tiles (rows 2^(a1 + w2) elements apart, a power of two of
+// megabytes) read at full speed from DRAM but poorly from L2, where such rows
+// crowd few L2 sets, while S2's rows (2^a1 elements apart) read from L2 at well
+// over twice DRAM speed. An S2 tile of slab v needs every S3 tile of slab v and
+// nothing else, so with the tasks ordered
+//   S3(slab 0 .. L-1), then S2(slab v) before S3(slab v + L), ...
+// S2 re-reads a slab that S3 wrote a few slabs earlier, while it is still in
+// L2 (S3 stores evict-last; at N = 28 complex64 a slab is 16 MB). DRAM sees S3's
+// reads and S2's writes only.
 //
 // Warp roles, one CTA per SM:
 //   warp 0 (producer): claims tasks one at a time from a global counter in
@@ -21,7 +26,7 @@
 //   warps 1-8 (the compute group, 256 threads): the rounds of a tile run
 //     between the group's named barrier; after the tile's last shared-memory
 //     read the group frees the stage (empty barrier) and stores straight from
-//     registers. An S2 tile then releases its slab counter (one thread,
+//     registers. An S3 tile then releases its slab counter (one thread,
 //     red.release.gpu after the group barrier that orders all the group's
 //     stores before it), deferred to the next tile's stage-free point so the
 //     group does not wait for its own stores to drain.
@@ -48,8 +53,8 @@ enum S23Kind : uint32_t { S23_S2 = 1, S23_S3 = 2, S23_END = 0xFF };
 
 // one launch = the strided part of one Trotter step
 struct S23Program {
-  // task order (claim index g -> task): for h = 0 .. slabs + lag - 1, the S2
-  // tiles of slab h (h < slabs), then the S3 tiles of slab h - lag (h >= lag),
+  // task order (claim index g -> task): for h = 0 .. slabs + lag - 1, the S3
+  // tiles of slab h (h < slabs), then the S2 tiles of slab h - lag (h >= lag),
   // 2^lb tiles each in increasing tile id; decoded in closed form (s23_decode)
   uint32_t slabs, lag, lb;          // slab count, S2 -> S3 lag in slabs, log2 tiles per slab and pass
   uint32_t x, y, mb2, bits;         // cpm - cp2, cpm - cp3, S2 mid bits, slab bits
@@ -57,7 +62,7 @@ struct S23Program {
   uint32_t step;                    // Trotter step (tangent index, slab-counter epoch)
   unsigned int* next;               // claim counter (reset by the last CTA to leave)
   unsigned int* ctas_done;
-  unsigned int* slab_done;          // S2 completions per slab, cumulative over the steps of a call
+  unsigned int* slab_done;          // S3 completions per slab, cumulative over the steps of a call
   int* err;
   int* abort;
   uint32_t poll_limit;
@@ -67,36 +72,38 @@ struct S23Task {
   uint32_t kind, slab, tile;
 };
 
-// Task g of the launch's claim order (g < n_tasks). S2 tiles of slab v are
+// Task g of the launch's claim order (g < n_tasks): per slab the S3 tiles first,
+// the S2 tiles `lag` slabs later. S2 tiles of slab v are
 // mid | hi << mb2 with mid = v << x | low; S3 tiles are low | v << y | up << (y + bits).
 __host__ __device__ inline S23Task s23_decode(const S23Program& P, uint32_t g) {
   const uint32_t B = 1u << P.lb;
-  uint32_t kind, v, i;
+  bool first;  // the slab's first sub-pass (S3) or its second (S2)
+  uint32_t v, i;
   if (g < P.lag * B) {
-    kind = S23_S2;
+    first = true;
     v = g >> P.lb;
     i = g & (B - 1u);
   } else {
     const uint32_t g1 = g - P.lag * B;
     if (g1 < 2u * B * (P.slabs - P.lag)) {
       const uint32_t pr = g1 >> (P.lb + 1u), r = g1 & (2u * B - 1u);
-      kind = r < B ? S23_S2 : S23_S3;
-      v = r < B ? P.lag + pr : pr;
+      first = r < B;
+      v = first ? P.lag + pr : pr;
       i = r & (B - 1u);
     } else {
       const uint32_t g2 = g1 - 2u * B * (P.slabs - P.lag);
-      kind = S23_S3;
+      first = false;
       v = P.slabs - P.lag + (g2 >> P.lb);
       i = g2 & (B - 1u);
     }
   }
   S23Task t;
-  t.kind = kind;
+  t.kind = first ? (uint32_t)S23_S3 : (uint32_t)S23_S2;
   t.slab = v;
-  if (kind == S23_S2)
-    t.tile = (v << P.x) | (i & ((1u << P.x) - 1u)) | ((i >> P.x) << P.mb2);
-  else
+  if (first)
     t.tile = (i & ((1u << P.y) - 1u)) | (v << P.y) | ((i >> P.y) << (P.y + P.bits));
+  else
+    t.tile = (v << P.x) | (i & ((1u << P.x) - 1u)) | ((i >> P.x) << P.mb2);
   return t;
 }
 
@@ -157,8 +164,8 @@ __global__ void __launch_bounds__(kS23Threads, 1)
       if (u > 0 && !s23_wait(smem_addr(&empty_bar[s]), (u - 1u) & 1u, P)) break;
       S23Task t{S23_END, 0u, 0u};
       if (ends == 0u && g < P.n_tasks && !s23_aborted(P)) t = s23_decode(P, g);
-      if (t.kind == S23_S3 && t.slab != ok_slab) {
-        // every S2 tile of the slab, this step, must be in memory
+      if (t.kind == S23_S2 && t.slab != ok_slab) {
+        // every S3 tile of the slab, this step, must be in memory
         const unsigned int* ctr = P.slab_done + t.slab;
         uint32_t polls = 0;
         bool ok = true;
@@ -188,7 +195,7 @@ __global__ void __launch_bounds__(kS23Threads, 1)
         mbar_arrive(fb);  // releases meta[s]; no bytes
       } else {
         StageMeta m;
-        m.kind = (t.kind == S23_S2) ? TASK_S2 : TASK_S3;
+        m.kind = (t.kind == S23_S2) ? TASK_S2 : TASK_S3;  // geometry of the tile
         m.inst = 0;
         m.tile = t.tile;
         m.step = P.step;
@@ -216,14 +223,14 @@ __global__ void __launch_bounds__(kS23Threads, 1)
   const uint32_t tg = tid - 32u - (uint32_t)kComputeThreads * grp;
   const GroupSync sy{1u + grp};
   const R t = D.tan[P.step];
-  // The release of an S2 tile's slab counter is deferred to the group's next
+  // The release of an S3 tile's slab counter is deferred to the group's next
   // stage-free point: a release makes the releasing thread wait until every
   // store it covers is performed, and by then the previous tile's stores have
   // had a whole tile's compute to drain, while the current tile's are not yet
   // issued. It is never held across a wait: if the next tile is not loaded yet
   // (its load may depend on this very slab), the release goes out first.
   // Only thread 0 of the group tracks it; the group barrier at the end of the
-  // S2 tile has made every thread's stores visible to it.
+  // S3 tile has made every thread's stores visible to it.
   constexpr uint32_t kNone = 0xFFFFFFFFu;
   uint32_t pending = kNone;
   for (uint32_t j = grp;; j += (uint32_t)kS23Groups) {
@@ -254,10 +261,10 @@ __global__ void __launch_bounds__(kS23Threads, 1)
     const uint32_t cp = (uint32_t)(kElemBits - w);
     const uint32_t mid = task.tile & ((1u << mb) - 1u), hi = task.tile >> mb;
     const uint32_t tile_base = (mid << cp) | (hi << (h0 + (uint32_t)w));
-    // S2 output is re-read by S3 from L2; S3 output streams to DRAM
+    // S3 (first) output is re-read by S2 from L2; S2 (second) output streams to DRAM
     process_s_dispatch<R>(w, stage, D.state, tile_base, h0, t, stage_free, tg, sy,
-                          s2 ? policy_evict_last() : policy_evict_first());
-    if (s2) {
+                          s2 ? policy_evict_first() : policy_evict_last());
+    if (!s2) {
       sy.sync();  // every store of the group's tile precedes the (deferred) release
       if (tg == 0) pending = task.slab;
     }
