@@ -1,10 +1,11 @@
-"""Engine mode 2: the A1 pass as a grid launch and both strided passes (S2, S3)
-as ONE persistent launch in which S3 re-reads, from L2, the slabs S2 has just
-written. Every element sees the same operations in the same order as with one
-launch per pass (mode 1), and the reductions are the same fixed-order sums, so
-the measured series must be bit-identical to mode 1 for every A1 kernel, S2
-width and slab lag; complex128 stays within 1e-10 of the oracle (the reference's
-step, src/sampling/sampler.cuh:604-618)."""
+"""Engine mode 2: the A1 pass as a grid launch and both strided passes as ONE
+persistent launch: the high-bit pass (S3) first, then the middle-bit pass (S2)
+re-reading from L2 the slabs S3 has just written. The Rx gates of different
+qubits commute, so this is the same step as one launch per pass (mode 1, S2
+then S3) up to the rounding of the other order: complex128 agrees with mode 1 to
+1e-12 and with the oracle to 1e-10 (the reference's step,
+src/sampling/sampler.cuh:604-618), complex64 within its parity bars; the slab lag
+only changes the schedule, so results are bit-identical across lags."""
 import numpy as np
 import pytest
 
@@ -49,12 +50,16 @@ CASES = [
 
 
 @pytest.mark.parametrize("n,precision,a1,w2", CASES)
-def test_fused_strided_equals_per_pass(eng, n, precision, a1, w2):
+def test_fused_strided_matches_per_pass(eng, n, precision, a1, w2):
     steps = 12 if n < 28 else 6
-    fused, _ = _run(eng, n, precision, 2, a1, w2, steps=steps)
-    per_pass, _ = _run(eng, n, precision, 1, a1, w2, steps=steps)
-    for a, b in zip(fused, per_pass):
-        assert np.array_equal(a, b), (n, precision, a1, w2)
+    (pf, df, nf), _ = _run(eng, n, precision, 2, a1, w2, steps=steps)
+    (pp, dp, np_), _ = _run(eng, n, precision, 1, a1, w2, steps=steps)
+    if precision == bk.BK_C128:
+        assert np.max(np.abs(pf - pp)) <= 1e-12 and np.max(np.abs(df - dp)) <= 1e-12 * n
+        assert np.max(np.abs(nf - np_)) <= 1e-12
+    else:
+        assert np.max(np.abs(pf - pp)) <= C64_DP_BAR and np.max(np.abs(df - dp)) <= C64_DH_BAR
+        assert np.max(np.abs(nf - np_)) <= 1e-5
 
 
 @pytest.mark.parametrize("lag", [1, 2, 8])
