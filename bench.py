@@ -64,6 +64,8 @@ def parse():
                     help="per-pass A1 kernel: 0 = 256x16, 1 = 512x8, 2 = warp-local (element bits 0-8), "
                          "3 = warp-local over 32 KB half tiles")
     ap.add_argument("--no-tune", action="store_true", help="engine defaults instead of the autotuner's choice")
+    ap.add_argument("--adjoint-config", choices=["standard", "large"], default="standard",
+                    help="adjoint workload: standard = N=22, 1280 steps; large = N=28, 2000 steps")
     ap.add_argument("--kernel-table-steps", type=int, default=3,
                     help="bench steps of the separate per-kernel timing pass (roofline)")
     return ap.parse_args()
@@ -393,16 +395,19 @@ def batched_cpu_baseline(inst, dt, per_n=2, steps=10):
 
 
 def run_adjoint(a):
-    """Adjoint gradient: N=22 trap (lowest 5% of 1000 descents), 64 segments g_j ~ U[0.25, 0.45], dt=0.02,
-    1280 steps, checkpoints every 128; one bench step = one bk_adjoint call (value and 64 gradients)."""
+    """Adjoint gradient. standard: N=22 trap (lowest 5% of 1000 descents), 64 segments g_j ~ U[0.25, 0.45],
+    dt=0.02, 1280 steps, checkpoints every 128. large: N=28 trap (lowest 1% of 4000 descents), 40 segments of
+    50 steps (2000 steps), checkpoint interval from bk_adjoint's free-memory rule. One bench step = one
+    bk_adjoint call (value and all segment gradients)."""
     import torch
     import bk_b200 as bk
-    n, nseg, T, K = 22, 64, 1280, 128
+    large = a.adjoint_config == "large"
+    n, nseg, T, K = (28, 40, 2000, 0) if large else (22, 64, 1280, 128)
     prec = bk.BK_C64 if a.precision == "c64" else bk.BK_C128
     dev = torch.device("cuda", 0)
     eng = bk.Engine(0)
-    bits, e0 = bk.select_trap(n, 42, 1000, 0.05)
-    gs = np.random.default_rng(42).uniform(0.25, 0.45, nseg)
+    bits, e0 = bk.select_trap(n, 42, 4000, 0.01) if large else bk.select_trap(n, 42, 1000, 0.05)
+    gs = np.random.default_rng(2028 if large else 42).uniform(0.25, 0.45, nseg)
     g_steps = np.repeat(gs, T // nseg)
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=dev)
     for _ in range(max(a.warmup, 1)):
@@ -440,27 +445,34 @@ def run_adjoint(a):
             "achieved": alg / rev_s / 1e9, "peak": peak, "unit": "GB/s", "frac": alg / rev_s / 1e9 / peak,
             "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg, "avg_launch_ms": 1e3 * rev_s,
             "traffic": None,
-            "l2": "psi and lambda are 32 MiB each at N = 22 complex64: both fit the 126 MB L2, so the HBM "
-                  "fraction is nominal"}
+            "l2": ("psi and lambda are 2 GiB each at N = 28 complex64, far above L2" if large else
+                   "psi and lambda are 32 MiB each at N = 22 complex64: both fit the 126 MB L2, so the HBM "
+                   "fraction is nominal")}
     cpu = None
     if not a.no_cpu_baseline:
         from oracle import oracle as O
         threads = os.cpu_count() or 1
-        Tc = 20
+        Tc = 2 if large else 20
         t0c = time.perf_counter()
         O.trotter_adjoint(n, bits, e0, g_steps[:Tc], a.dt, Tc, threads=threads)
         secs = time.perf_counter() - t0c
         cpu = {"value": float(1 << n) * Tc / secs, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"forward + adjoint gradient of {Tc} steps of the same N=22 trap and schedule by the "
+               "sample": f"forward + adjoint gradient of {Tc} steps of the same N={n} trap and schedule by the "
                          f"oracle (complex128, exact gates, sqrt(T) checkpoints), {secs:.1f} s"}
-    line = {"metric": "Adjoint gradient amp-steps/s (N=22, 64 segments, 1280 steps; forward + reverse sweep)",
+    cfg_name = (f"N={n}, {nseg} segments, {T} steps" + (", checkpoints sized to free HBM" if large else ""))
+    line = {"metric": f"Adjoint gradient amp-steps/s ({cfg_name}; forward + reverse sweep)",
             "value": amp_steps * a.steps / dev_s, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1e3 * dev_s / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": a.precision, "data": "synthetic (seeded trap and field schedule, no dataset)",
-            "config": {"workload": "N=22 trap (lowest 5% of 1000 descents, seed 42), 64 segments g_j ~ U[0.25, 0.45] "
-                                   "(seed 42), dt=0.02, 1280 steps, checkpoints every 128, objective P_<(T)",
-                       "n": n, "segments": nseg, "trotter_steps": T, "checkpoint_every": K,
-                       "l2": "two 32 MiB statevectors (complex64) fit the 126 MB L2"},
+            "config": {"workload": (f"N={n} trap (lowest 1% of 4000 descents, seed 42), {nseg} segments g_j ~ "
+                                    "U[0.25, 0.45] (seed 2028), dt=0.02, 2000 steps, checkpoint interval from the "
+                                    "free-memory rule, objective P_<(T)") if large else
+                                   ("N=22 trap (lowest 5% of 1000 descents, seed 42), 64 segments g_j ~ U[0.25, 0.45] "
+                                    "(seed 42), dt=0.02, 1280 steps, checkpoints every 128, objective P_<(T)"),
+                       "n": n, "segments": nseg, "trotter_steps": T, "checkpoint_every": st["checkpoint_every"],
+                       "n_checkpoints": st["n_checkpoints"],
+                       "l2": ("statevectors of 2 GiB (complex64) each, far above the 126 MB L2" if large else
+                              "two 32 MiB statevectors (complex64) fit the 126 MB L2")},
             "compare": {"forward_ms": 1e3 * fwd_s, "gradient_ms": 1e3 * dev_s / a.steps,
                         "gradient_cost_in_forwards": dev_s / a.steps / fwd_s,
                         "reverse_over_forward": float(np.mean(rv)) / float(np.mean(fw)),
