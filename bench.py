@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--a1-kernel", type=int, default=None, choices=[0, 1, 2, 3],
                     help="per-pass A1 kernel: 0 = 256x16, 1 = 512x8, 2 = warp-local (element bits 0-8), "
                          "3 = warp-local over 32 KB half tiles")
+    ap.add_argument("--phase-table", type=int, default=None, choices=[0, 1],
+                    help="complex64 A1 kernels 1-3: 1 = the full per-energy phase table")
     ap.add_argument("--no-tune", action="store_true", help="engine defaults instead of the autotuner's choice")
     ap.add_argument("--adjoint-config", choices=["standard", "large"], default="standard",
                     help="adjoint workload: standard = N=22, 1280 steps; large = N=28, 2000 steps")
@@ -269,7 +271,8 @@ def tuned_knobs(eng, a, n, prec, trap):
     for this device and size, else a tuning sweep now (not timed, not cached)."""
     from bk_b200 import tune
     explicit = {k: v for k, v in (("engine_mode", a.engine_mode), ("slab_lag", a.slab_lag),
-                                  ("split_w2", a.split_w2), ("a1_wide", a.a1_kernel)) if v is not None}
+                                  ("split_w2", a.split_w2), ("a1_wide", a.a1_kernel),
+                                  ("phase_table", a.phase_table)) if v is not None}
     if explicit or a.no_tune:
         for k, v in explicit.items():
             eng.set_option(k, v)

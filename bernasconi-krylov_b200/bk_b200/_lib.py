@@ -460,7 +460,7 @@ class Engine:
         return out
 
     OPTIONS = {"engine_mode": 0, "slab_lag": 1, "split_w2": 2, "e_source": 3, "a1_wide": 4, "adj_a1": 5,
-               "wait_polls": 6, "test_hold_step": 7}
+               "wait_polls": 6, "test_hold_step": 7, "phase_table": 8}
 
     def set_option(self, name, value):
         self._check(self.L.bk_set_option(self.ctx, self.OPTIONS[name], int(value)), "bk_set_option")

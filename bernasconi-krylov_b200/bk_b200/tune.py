@@ -15,7 +15,11 @@ Knobs (engine options, include/bk_engine.h):
                (element bits 0-11), 1 = 512 x 8, 2 = warp-local (element bits
                0-8 inside each warp, no CTA barrier; the strided passes take
                bits 9 and up; up to 27 element bits), 3 = warp-local with
-               4-warp CTAs over 32 KB half tiles (four CTAs per SM).
+               4-warp CTAs over 32 KB half tiles (four CTAs per SM);
+  phase_table  complex64 per-pass A1 kernels 1-3: 1 = the diagonal phase of
+               each energy level from a full table (E = floor(n/2) mod 4 for
+               every LABS energy) as two half-angle shear rotations, 0 = level
+               table and residual polynomials.
 For the batched engine the knob is the task-block lag between a statevector
 slab's A1 and S2 tasks.
 
@@ -34,8 +38,8 @@ import os
 from ._lib import BK_C64, BK_C128
 
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.json")
-KNOBS = ("engine_mode", "slab_lag", "split_w2", "e_source", "a1_wide")
-DEFAULTS = {"engine_mode": 0, "slab_lag": 3, "split_w2": 0, "e_source": 0, "a1_wide": 0}
+KNOBS = ("engine_mode", "slab_lag", "split_w2", "e_source", "a1_wide", "phase_table")
+DEFAULTS = {"engine_mode": 0, "slab_lag": 3, "split_w2": 0, "e_source": 0, "a1_wide": 0, "phase_table": 0}
 ELEM_BITS = 12  # element bits of one 64 KB tile
 
 
@@ -87,6 +91,9 @@ def candidates(n, precision):
     fused(rest, widths, (0, 1))
     if 1 <= rest9 <= 18:
         fused(rest9, [0] + [w for w in (d9 - 1, d9 + 1) if 3 <= w <= 9 and w <= rest9 and rest9 - w <= 9], (2, 3))
+    # complex64: the full phase table with every per-pass candidate whose A1 kernel takes it (1-3)
+    if precision == BK_C64:
+        out += [dict(c, phase_table=1) for c in list(out) if c["engine_mode"] in (1, 2) and c["a1_wide"] >= 1]
     # E recomputed in the pass, on the default split of both schedules
     out.append(dict(engine_mode=1, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))
     out.append(dict(engine_mode=0, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))

@@ -97,6 +97,7 @@ struct bk_ctx {
   int force_w2 = 0;           // S2 width when > 0 and valid for the size (else the default split)
   int e_recompute = 0;        // tile engine: 1 = E(s) recomputed from popcounts in A1, 0 = uint16 table
   int a1_wide = 0;            // per-pass schedule A1: 1 = 512 threads x 8 elements, 2 = warp-local (bits 0-8)
+  int phase_table = 0;        // complex64 per-pass A1 (kernels 1-3): 1 = the full per-energy phase table
   int adj_a1 = 0;             // adjoint reverse sweep A1: 0 = 12-bit, 1 = warp-local (element bits 0-8)
   uint32_t wait_polls = 0;    // persistent engine: polls of a dependency wait before it gives up (0 = default)
   uint64_t s23_checked = 0;   // fused strided pass geometry (np, a1, w2, lag) whose closed form was checked
@@ -570,6 +571,27 @@ int build_phase_v(bk_ctx* c, int n, double angle_unit, PhaseV32* P, std::vector<
   return BK_OK;
 }
 
+// complex64 full phase table of the looping A1: every LABS energy is
+// E = c0 + 4 j with c0 = floor(n/2) mod 4 (C_k has the parity of n - k, and an
+// odd square is 1 mod 8, an even one 0 mod 4), so j < (Emax - c0) / 4 + 1 indexes
+// every level; tab[j] = {-tan(r/4), sin(r/2)} for r = -angle_unit E reduced to
+// (-pi, pi], applied as two half-angle shear rotations.
+int build_phase_table(bk_ctx* c, int n, double angle_unit, PhaseV32* P, std::vector<float2>* tab) {
+  const int emax = (n - 1) * n * (2 * n - 1) / 6;
+  const int c0 = (n / 2) & 3;
+  const int n_j = (emax - c0) / 4 + 1;
+  if (n_j > kPhaseTabMax) return fail(c, BK_ERR_UNSUPPORTED, "phase table of %d entries for n = %d", n_j, n);
+  tab->assign((size_t)((n_j + 1) & ~1), make_float2(0.f, 0.f));  // even count: the copy is a 16-byte multiple
+  const double two_pi = 6.283185307179586;
+  for (int j = 0; j < n_j; ++j) {
+    const double r = std::remainder(-angle_unit * (double)(c0 + 4 * j), two_pi);  // [-pi, pi]
+    (*tab)[(size_t)j] = make_float2((float)(-std::tan(0.25 * r)), (float)std::sin(0.5 * r));
+  }
+  P->c0 = c0;
+  P->n_j = n_j;
+  return BK_OK;
+}
+
 // bump allocator over the context's persistent-engine buffer (256-byte aligned pieces)
 struct Bump {
   size_t off = 0;
@@ -600,6 +622,7 @@ struct PersistRun {
   uint32_t slabs23 = 0;
   S23Program prog23{};            // the task order's closed form (counters set at launch)
   unsigned int* ctr23 = nullptr;  // [slab_done: slabs23][next][ctas_done][abort]
+  bool a1_table = false;          // the A1 pass takes its phase from the full table (complex64)
 };
 
 // Slab of a strided tile for the fused S2 + S3 pass: the element bits
@@ -621,6 +644,28 @@ int split_w2(const bk_ctx* c, int rest) {
   const int w = c->force_w2;
   if (w >= 1 && w <= 9 && w <= rest && rest - w <= 9) return w;
   return (rest <= 9) ? rest : (rest + 1) / 2;
+}
+
+// complex64 per-pass A1 kernels with the full phase table (complex128 has none)
+template <class R>
+int allow_table_a1(bk_ctx* c) {
+  if constexpr (sizeof(R) == 4) {
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_wide_kernel<R, true>), A1Smem<true>::kBytes));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 8, true>), WarpA1Smem<8, true>::kBytes));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 4, true>), WarpA1Smem<4, true>::kBytes));
+  }
+  return BK_OK;
+}
+template <class R>
+void launch_table_a1(const InstDesc<R>& D, int a1_wide, uint32_t n_a1, cudaStream_t st, uint32_t step, int* err) {
+  if constexpr (sizeof(R) == 4) {
+    if (D.a1_bits == kA1WarpBits && a1_wide == 3)
+      tile_a1_warp_kernel<R, 4, true><<<2 * n_a1, 128, WarpA1Smem<4, true>::kBytes, st>>>(D, step, err);
+    else if (D.a1_bits == kA1WarpBits)
+      tile_a1_warp_kernel<R, 8, true><<<n_a1, kComputeThreads, WarpA1Smem<8, true>::kBytes, st>>>(D, step, err);
+    else
+      tile_a1_wide_kernel<R, true><<<n_a1, kA1WideThreads, A1Smem<true>::kBytes, st>>>(D, step, err);
+  }
 }
 
 template <class R>
@@ -658,8 +703,12 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   typename PhaseV<R>::params ph{};
   std::vector<float2> hab;
   std::vector<double2> t64;
+  std::vector<float2> ptab;
   if constexpr (sizeof(R) == 4) {
     BK_TRY(build_phase_v(c, n, angle_unit, &ph, &hab));
+    // the full phase table for the per-pass 512-thread and warp-local A1 kernels
+    if (grid_mode && c->phase_table && (c->a1_wide == 1 || a1_warp))
+      BK_TRY(build_phase_table(c, n, angle_unit, &ph, &ptab));
   } else {
     Phase64 p64{};
     BK_TRY(build_phase(c, n, angle_unit, &p64));  // uploads to d_phase
@@ -702,6 +751,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   const size_t o_scale = b.take(std::max<size_t>(scales.size(), 1) * sizeof(R));
   const size_t o_slot = b.take(S.slot.size() * sizeof(int));
   const size_t o_hab = b.take(std::max<size_t>(hab.size(), 1) * sizeof(float2));
+  const size_t o_ptab = b.take(std::max<size_t>(ptab.size(), 1) * sizeof(float2));
   const size_t o_ctr = b.take((slabs + 8) * sizeof(unsigned int));
   const size_t o_part = b.take(3 * (size_t)n_a1 * (a1_half ? 2 : 1) * sizeof(double));
   // fused strided pass: tasks in slab order (S2 of slab h after S3 of slab h + lag)
@@ -791,7 +841,10 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   D.s3_mid_bits = w3 > 0 ? (int)m3.mid_bits : 0;
   D.e0 = (int)p->e0;
   D.s0 = (uint32_t)(p->s0 & ((1ull << n) - 1ull));
-  if constexpr (sizeof(R) == 4) ph.hab = reinterpret_cast<const float2*>(base + o_hab);
+  if constexpr (sizeof(R) == 4) {
+    ph.hab = reinterpret_cast<const float2*>(base + o_hab);
+    if (!ptab.empty()) ph.tab = reinterpret_cast<const float2*>(base + o_ptab);
+  }
   D.phase = ph;
   D.tan = reinterpret_cast<const R*>(base + o_tan);
   D.scale = reinterpret_cast<const R*>(base + o_scale);
@@ -823,6 +876,8 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   BK_CUDA(c, cudaMemcpyAsync(base + o_slot, S.slot.data(), S.slot.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   if (!hab.empty())
     BK_CUDA(c, cudaMemcpyAsync(base + o_hab, hab.data(), hab.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
+  if (!ptab.empty())
+    BK_CUDA(c, cudaMemcpyAsync(base + o_ptab, ptab.data(), ptab.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
   if (prog23.n_tasks > 0) BK_CUDA(c, cudaMemsetAsync(base + o_ctr23, 0, (slabs23 + 4) * sizeof(unsigned int), st));
   BK_TRY(allow_smem(c, reinterpret_cast<const void*>(persist_kernel<R, true>), PersistSmem::kBytes));
   run->base = base;
@@ -848,6 +903,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   run->slabs23 = slabs23;
   run->prog23 = prog23;
   run->ctr23 = reinterpret_cast<unsigned int*>(base + o_ctr23);
+  run->a1_table = !ptab.empty();
   return BK_OK;
 }
 
@@ -923,9 +979,14 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
       P23.poll_limit = c->wait_polls > 0 ? c->wait_polls : kWaitPolls * 4u;
     }
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_pass_kernel<R>), PersistSmem::kBytes));
-    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_wide_kernel<R>), PersistSmem::kBytes));
-    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 8>), kA1WarpSmem));
-    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 4>), HalfA1Smem::kBytes));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_wide_kernel<R, false>), A1Smem<false>::kBytes));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 8, false>),
+                      WarpA1Smem<8, false>::kBytes));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 4, false>),
+                      WarpA1Smem<4, false>::kBytes));
+    // the full phase table (complex64 A1 kernels 1-3)
+    const bool a1_table = run.a1_table;
+    if (a1_table) BK_TRY(allow_table_a1<R>(c));
     using SampT = typename std::conditional<sizeof(R) == 4, Planar64, double2>::type;
     BK_CUDA(c, cudaMemsetAsync(ctr, 0, (slabs + 8) * sizeof(unsigned int), st));
     for (int k = 0; k <= p->n_steps; ++k) {
@@ -942,12 +1003,15 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
         break;
       }
       BK_TRY(ev_begin(c, "tile_a1", &ev));
-      if (D.a1_bits == kA1WarpBits && c->a1_wide == 3)
-        tile_a1_warp_kernel<R, 4><<<2 * n_a1, 128, HalfA1Smem::kBytes, st>>>(D, (uint32_t)k, err);
+      if (a1_table)
+        launch_table_a1(D, c->a1_wide, n_a1, st, (uint32_t)k, err);
+      else if (D.a1_bits == kA1WarpBits && c->a1_wide == 3)
+        tile_a1_warp_kernel<R, 4, false><<<2 * n_a1, 128, WarpA1Smem<4, false>::kBytes, st>>>(D, (uint32_t)k, err);
       else if (D.a1_bits == kA1WarpBits)
-        tile_a1_warp_kernel<R, 8><<<n_a1, kComputeThreads, kA1WarpSmem, st>>>(D, (uint32_t)k, err);
+        tile_a1_warp_kernel<R, 8, false><<<n_a1, kComputeThreads, WarpA1Smem<8, false>::kBytes, st>>>(D, (uint32_t)k,
+                                                                                                     err);
       else if (c->a1_wide == 1)
-        tile_a1_wide_kernel<R><<<n_a1, kA1WideThreads, PersistSmem::kBytes, st>>>(D, (uint32_t)k, err);
+        tile_a1_wide_kernel<R, false><<<n_a1, kA1WideThreads, A1Smem<false>::kBytes, st>>>(D, (uint32_t)k, err);
       else
         tile_pass_kernel<R><<<n_a1, kComputeThreads, PersistSmem::kBytes, st>>>(D, TASK_A1, (uint32_t)k, err);
       BK_CUDA(c, cudaGetLastError());
@@ -2112,6 +2176,10 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
         return fail(c, BK_ERR_INVALID, "wait polls %lld", (long long)value);
       c->wait_polls = (uint32_t)value;
       return BK_OK;
+    case BK_OPT_PHASE_TABLE:
+      if (value != 0 && value != 1) return fail(c, BK_ERR_INVALID, "phase table %lld", (long long)value);
+      c->phase_table = (int)value;
+      return BK_OK;
     case BK_OPT_TEST_HOLD_STEP:
       if (value < -1 || value > (int64_t)1 << 30) return fail(c, BK_ERR_INVALID, "hold step %lld", (long long)value);
       c->hold_step = value;
@@ -2132,6 +2200,7 @@ int bk_get_option(const bk_ctx* c, int option, int64_t* value) {
     case BK_OPT_ADJ_A1: *value = c->adj_a1; return BK_OK;
     case BK_OPT_WAIT_POLLS: *value = c->wait_polls; return BK_OK;
     case BK_OPT_TEST_HOLD_STEP: *value = c->hold_step; return BK_OK;
+    case BK_OPT_PHASE_TABLE: *value = c->phase_table; return BK_OK;
     default: return BK_ERR_INVALID;
   }
 }

@@ -51,12 +51,6 @@ __global__ void __launch_bounds__(kFsThreads) fs_pass_kernel(const double* __res
   }
 }
 
-// 1-D bulk copy global -> this CTA's shared memory (16-byte aligned, size a multiple of 16), completion on `bar`
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
 
 constexpr int kFsPer = (1 << kFsTileBits) / kFsThreads;  // 32 tile positions per thread
 

@@ -139,6 +139,10 @@ struct PhaseV32 {
   uint32_t K, M;      // h = umulhi(E, M)
   float theta, theta_lo;
   int n_h;
+  // full table (BK_OPT_PHASE_TABLE): tab[j] = {-tan(r_j/4), sin(r_j/2)} for
+  // E = c0 + 4 j (every LABS energy is floor(n/2) mod 4), padded to an even count
+  const float2* tab;  // [n_j rounded up to even]
+  int c0, n_j;
 };
 struct PhaseV64 {
   const double2* hi;  // [n_hi] (cos, sin)(theta 128 h)
@@ -663,10 +667,11 @@ __device__ __forceinline__ const unsigned int* task_dep(const InstDesc<R>& D, co
 
 template <class R>
 __device__ __forceinline__ void issue_task_load(const InstDesc<R>& D, const StageMeta& m, unsigned char* stage,
-                                                uint32_t fb) {
+                                                uint32_t fb, uint32_t extra_tx = 0u) {
   if (m.kind == TASK_A1 || m.kind == TASK_M) {
     const bool e_tile = !D.e_recompute;
-    mbar_arrive_expect_tx(fb, (uint32_t)kStageTileBytes + (e_tile ? 4096u * 2u * (uint32_t)El<R>::kAmps : 0u));
+    mbar_arrive_expect_tx(fb, (uint32_t)kStageTileBytes + (e_tile ? 4096u * 2u * (uint32_t)El<R>::kAmps : 0u) +
+                                  extra_tx);
     const int hd = D.a1_hi_dim;
     const uint64_t pol = policy_evict_first();
     tma_load_5d_hint(smem_addr(stage), D.map_a1, 0, 0, hd == 2 ? (int)m.tile : 0, hd == 3 ? (int)m.tile : 0, 0, fb,
@@ -854,6 +859,52 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
 }
 
 // ---------------------------------------------------------------------------
+// Full phase table (BK_OPT_PHASE_TABLE, complex64 per-pass A1 kernels): every
+// LABS energy is E = c0 + 4 j with c0 = floor(n/2) mod 4, so one table entry
+// {-tan(r/4), sin(r/2)} per level j (r = theta E reduced to (-pi, pi]) gives the
+// rotation as two half-angle shear rotations: no level split and no residual
+// polynomial, a third of the phase's FMA work. The table (at most 2139 entries,
+// 17 KB at n = 30) arrives by one bulk copy on the tile's own barrier.
+// ---------------------------------------------------------------------------
+constexpr int kPhaseTabMax = 2144;  // >= (8555 - 3) / 4 + 1 entries at n = 30, even
+constexpr int kPhaseTabBytes = kPhaseTabMax * (int)sizeof(float2);
+static_assert(kPhaseTabBytes >= 3328, "the table room also holds the level tables");
+
+// bytes of the table copy (the count rounded up to an even number of entries: 16-byte multiple)
+__device__ __forceinline__ uint32_t phase_tab_bytes(const PhaseV32& P) {
+  return (uint32_t)((P.n_j + 1) & ~1) * (uint32_t)sizeof(float2);
+}
+
+// the full-table rotation of a complex64 element (two amplitudes, energies packed in e2)
+__device__ __forceinline__ void phase_table_apply(El<float>::T& v, uint32_t e2, const unsigned char* s,
+                                                  uint32_t c0) {
+  const float2* tab = reinterpret_cast<const float2*>(s);
+  const uint32_t j0 = ((e2 & 0xFFFFu) - c0) >> 2, j1 = ((e2 >> 16) - c0) >> 2;
+  const float2 H0 = tab[j0], H1 = tab[j1];
+  const float2 A = make_float2(H0.x, H1.x), B = make_float2(H0.y, H1.y);
+  PhaseV<float>::shear2(v.re, v.im, A, B);
+  PhaseV<float>::shear2(v.re, v.im, A, B);
+}
+
+// the A1 kernels' phase: the full table (kTab, complex64) or the level table with residual polynomials
+template <class R, bool kTab>
+__device__ __forceinline__ void a1_phase(typename El<R>::T& v, uint32_t e, const InstDesc<R>& D,
+                                         const unsigned char* phase_smem) {
+  if constexpr (kTab)
+    phase_table_apply(v, e, phase_smem, (uint32_t)D.phase.c0);
+  else
+    PhaseV<R>::apply(v, e, D.phase, phase_smem, false);
+}
+
+// shared memory of a 64 KB-tile A1 kernel: the stage, the phase room, reduction scratch
+template <bool kTab>
+struct A1Smem {
+  static constexpr int kPhaseOff = PersistSmem::kStageBytes;
+  static constexpr int kRedOff = kPhaseOff + (kTab ? kPhaseTabBytes : 3328);
+  static constexpr int kBytes = kRedOff + 512;
+};
+
+// ---------------------------------------------------------------------------
 // Wide A1 for the per-pass schedule: 512 threads x 8 elements per tile, so 32
 // warps share an SM (two CTAs) instead of 16 — more latency hiding for the
 // diagonal phase, the pass's dominant cost. Four rounds of 3 register bits
@@ -894,18 +945,20 @@ __device__ __forceinline__ void el8_bflys(typename El<R>::T (&v)[8], R t) {
   }
 }
 
-template <class R>
+template <class R, bool kTab>
 __global__ void __launch_bounds__(kA1WideThreads, 2)
     tile_a1_wide_kernel(const __grid_constant__ InstDesc<R> D, uint32_t step, int* err) {
+  static_assert(!kTab || sizeof(R) == 4, "the full phase table is complex64 only");
   using PL = PlanA1Wide;
   using E = El<R>;
+  using SM = A1Smem<kTab>;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t full_bar;
   __shared__ int last_flag;
   unsigned char* tile = smem;
   const unsigned char* etile = smem + kStageTileBytes;
-  unsigned char* phase_smem = smem + PersistSmem::kPhaseOff;
-  double* red = reinterpret_cast<double*>(smem + PersistSmem::kRedOff);
+  unsigned char* phase_smem = smem + SM::kPhaseOff;
+  double* red = reinterpret_cast<double*>(smem + SM::kRedOff);
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t fb = smem_addr(&full_bar);
   const uint32_t t_idx = blockIdx.x;
@@ -918,9 +971,15 @@ __global__ void __launch_bounds__(kA1WideThreads, 2)
   if (tid == 0) {
     mbar_init(fb, 1);
     fence_barrier_init();
-    issue_task_load(D, m, tile, fb);
+    if constexpr (kTab) {
+      const uint32_t tb = phase_tab_bytes(D.phase);
+      issue_task_load(D, m, tile, fb, tb);
+      bulk_load(smem_addr(phase_smem), D.phase.tab, tb, fb);
+    } else {
+      issue_task_load(D, m, tile, fb);
+    }
   }
-  PhaseV<R>::stage(D.phase, phase_smem, (int)tid, kA1WideThreads);
+  if constexpr (!kTab) PhaseV<R>::stage(D.phase, phase_smem, (int)tid, kA1WideThreads);
   __syncthreads();
   const bool ok = mbar_wait_bounded(fb, 0, err);
   if (__syncthreads_or(!ok)) return;
@@ -935,7 +994,7 @@ __global__ void __launch_bounds__(kA1WideThreads, 2)
     const uint32_t i = b1 | pdep((uint32_t)j, PL::R1_REG);
     const uint32_t e = D.e_recompute ? recompute_e<R>(tile_base | i, D.n) : load_e<R>(etile, i);
     if (slot >= 0) measure_el(acc, v[j], e, tile_base | i, D.e0, D.s0);
-    PhaseV<R>::apply(v[j], e, D.phase, phase_smem, false);
+    a1_phase<R, kTab>(v[j], e, D, phase_smem);
     E::bfly_inner(v[j], t);
   }
   const R sc = D.scale[step];
@@ -1071,18 +1130,32 @@ struct HalfA1Smem {
 // (2048 elements, 32 KB; four CTAs per SM instead of two, so more independent
 // load -> compute -> store chains overlap on each SM). Each warp owns a 512-element
 // block either way: same arithmetic per element, bit-identical results.
-template <class R, int NW>
+// shared memory of the warp-local A1 (NW warps; kTab: room for the full phase
+// table), + room to align the stage to 1024 bytes
+template <int NW, bool kTab>
+struct WarpA1Smem {
+  static constexpr int kEOff = (NW == 8) ? kStageTileBytes : HalfA1Smem::kEOff;
+  static constexpr int kPhaseOff = (NW == 8) ? PersistSmem::kPhaseOff : HalfA1Smem::kPhaseOff;
+  static constexpr int kRedOff = kPhaseOff + (kTab ? kPhaseTabBytes : 3328);
+  static constexpr int kBytes = kRedOff + 512 + 1024;
+};
+static_assert(WarpA1Smem<8, false>::kBytes == kA1WarpSmem && WarpA1Smem<4, false>::kBytes == HalfA1Smem::kBytes,
+              "the warp-local layouts without the table are the original ones");
+
+template <class R, int NW, bool kTab>
 __global__ void __launch_bounds__(NW * 32, 8 / NW * 2)
     tile_a1_warp_kernel(const __grid_constant__ InstDesc<R> D, uint32_t step, int* err) {
   using PL = PlanA1Warp;
   using E = El<R>;
   static_assert(NW == 8 || NW == 4, "");
+  static_assert(!kTab || sizeof(R) == 4, "the full phase table is complex64 only");
   constexpr int kTB = kA1WarpBits + (NW == 8 ? 3 : 2);   // element bits of the CTA's tile
   constexpr uint32_t kWarpMask = (NW == 8) ? PL::WARP : 0x600u;
   constexpr uint32_t kTileBytes = 16u << kTB;
-  constexpr int kEOff = (NW == 8) ? kStageTileBytes : HalfA1Smem::kEOff;
-  constexpr int kPhaseOff = (NW == 8) ? PersistSmem::kPhaseOff : HalfA1Smem::kPhaseOff;
-  constexpr int kRedOff = (NW == 8) ? PersistSmem::kRedOff : HalfA1Smem::kRedOff;
+  using SM = WarpA1Smem<NW, kTab>;
+  constexpr int kEOff = SM::kEOff;
+  constexpr int kPhaseOff = SM::kPhaseOff;
+  constexpr int kRedOff = SM::kRedOff;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar;
   __shared__ int last_flag;
@@ -1100,7 +1173,10 @@ __global__ void __launch_bounds__(NW * 32, 8 / NW * 2)
     mbar_init(fb, 1);
     fence_barrier_init();
     const bool e_tile = !D.e_recompute;
-    mbar_arrive_expect_tx(fb, kTileBytes + (e_tile ? (kTileBytes / 16u) * 2u * (uint32_t)E::kAmps : 0u));
+    uint32_t tb = 0u;
+    if constexpr (kTab) tb = phase_tab_bytes(D.phase);
+    mbar_arrive_expect_tx(fb, kTileBytes + (e_tile ? (kTileBytes / 16u) * 2u * (uint32_t)E::kAmps : 0u) + tb);
+    if constexpr (kTab) bulk_load(smem_addr(phase_smem), D.phase.tab, tb, fb);
     const uint64_t pol = policy_evict_first();
     if constexpr (NW == 8) {
       tma_load_5d_hint(smem_addr(tile), D.map_a1s, 0, 0, 0, (int)t_idx, 0, fb, pol);
@@ -1111,7 +1187,7 @@ __global__ void __launch_bounds__(NW * 32, 8 / NW * 2)
       if (e_tile) tma_load_5d_hint(smem_addr(tile + kEOff), D.map_e_half, 0, 0, (int)t_idx, 0, 0, fb, pol);
     }
   }
-  PhaseV<R>::stage(D.phase, phase_smem, (int)tid, NW * 32);
+  if constexpr (!kTab) PhaseV<R>::stage(D.phase, phase_smem, (int)tid, NW * 32);
   __syncthreads();
   const bool ok = mbar_wait_bounded(fb, 0, err);
   if (__syncthreads_or(!ok)) return;
@@ -1141,7 +1217,7 @@ __global__ void __launch_bounds__(NW * 32, 8 / NW * 2)
     for (int q = 0; q < 8; ++q) {
       const int j = 8 * h + q;
       if (slot >= 0) measure_el(acc, v[j], ev[q], tile_base | eb | (uint32_t)q, D.e0, D.s0);
-      PhaseV<R>::apply(v[j], ev[q], D.phase, phase_smem, false);
+      a1_phase<R, kTab>(v[j], ev[q], D, phase_smem);
       E::bfly_inner(v[j], t);
     }
   }

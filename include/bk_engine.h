@@ -297,7 +297,13 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       persistent engine (BK_OPT_ENGINE_MODE 0), the A1 tasks of this step of a
  *       launch wait for one completion more than can arrive, as if a producer
  *       were lost; the bounded wait runs out, every CTA leaves, and bk_evolve
- *       returns BK_ERR_TIMEOUT with the context still usable. */
+ *       returns BK_ERR_TIMEOUT with the context still usable;
+ *   BK_OPT_PHASE_TABLE: complex64, per-pass schedules (modes 1 and 2) with the
+ *       A1 kernels 1-3: 1 = the diagonal phase of every energy level from one
+ *       table entry (E = floor(n/2) mod 4 for every LABS energy, so at most 2139
+ *       levels, 17 KB) applied as two half-angle shear rotations; 0 (default) =
+ *       a 16-entry level table and residual polynomials. Other kernels and
+ *       complex128 ignore it. */
 enum {
   BK_OPT_ENGINE_MODE = 0,
   BK_OPT_SLAB_LAG = 1,
@@ -306,7 +312,8 @@ enum {
   BK_OPT_A1_WIDE = 4,
   BK_OPT_ADJ_A1 = 5,
   BK_OPT_WAIT_POLLS = 6,
-  BK_OPT_TEST_HOLD_STEP = 7
+  BK_OPT_TEST_HOLD_STEP = 7,
+  BK_OPT_PHASE_TABLE = 8
 };
 int bk_set_option(bk_ctx* ctx, int option, int64_t value);
 int bk_get_option(const bk_ctx* ctx, int option, int64_t* value);

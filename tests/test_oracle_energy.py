@@ -141,3 +141,26 @@ def test_oracle_matches_reference_build():
         for s in a[:40]:
             assert O.steepest_descent(n, int(s)) == O.steepest_descent(n, int(s), use_ref=True)
             assert O.steepest_descent(n, int(s), 3 * n) == O.steepest_descent(n, int(s), 3 * n, use_ref=True)
+
+
+def test_energy_levels_fit_the_full_phase_table():
+    """The complex64 A1 kernels' full phase table (BK_OPT_PHASE_TABLE) indexes the
+    level j = (E - c0) / 4 with c0 = floor(n/2) mod 4: C_k has the parity of n - k,
+    an odd square is 1 mod 8 and an even one 0 mod 4, so every energy is c0 mod 4
+    and at least c0. Checked on every state of n = 3..20 (the oracle's energy table,
+    the restatement of labs_energy.hpp:121-149), and the table capacity compiled
+    into the kernels (kPhaseTabMax) against the largest padded count, n = 30."""
+    import os
+    import re
+    for n in range(3, 21):
+        E = O.energy_table(n).astype(np.int64)
+        c0 = (n // 2) & 3
+        emax = (n - 1) * n * (2 * n - 1) // 6
+        assert np.all(E % 4 == c0) and E.min() >= c0 and E.max() <= emax, n
+    src = open(os.path.join(os.path.dirname(__file__), "..", "bernasconi-krylov_b200", "csrc",
+                            "bk_persist.cuh")).read()
+    cap = int(re.search(r"constexpr int kPhaseTabMax = (\d+);", src).group(1))
+    for n in range(14, 31):
+        emax = (n - 1) * n * (2 * n - 1) // 6
+        n_j = (emax - ((n // 2) & 3)) // 4 + 1
+        assert ((n_j + 1) & ~1) <= cap, n
