@@ -383,22 +383,6 @@ __device__ __forceinline__ double adj_s(unsigned char* sp, unsigned char* sl, co
   return acc;
 }
 
-template <class R, class F>
-__device__ __forceinline__ double adj_s_dispatch(int w, unsigned char* sp, unsigned char* sl, const AdjDesc<R>& D,
-                                                 uint32_t tile_base, uint32_t h0, uint32_t j, int m0, F&& f) {
-  switch (w) {
-    case 1: return adj_s<R, 1>(sp, sl, D, tile_base, h0, j, m0, f);
-    case 2: return adj_s<R, 2>(sp, sl, D, tile_base, h0, j, m0, f);
-    case 3: return adj_s<R, 3>(sp, sl, D, tile_base, h0, j, m0, f);
-    case 4: return adj_s<R, 4>(sp, sl, D, tile_base, h0, j, m0, f);
-    case 5: return adj_s<R, 5>(sp, sl, D, tile_base, h0, j, m0, f);
-    case 6: return adj_s<R, 6>(sp, sl, D, tile_base, h0, j, m0, f);
-    case 7: return adj_s<R, 7>(sp, sl, D, tile_base, h0, j, m0, f);
-    case 8: return adj_s<R, 8>(sp, sl, D, tile_base, h0, j, m0, f);
-    default: return adj_s<R, 9>(sp, sl, D, tile_base, h0, j, m0, f);
-  }
-}
-
 template <class R, bool kWarpA1>
 __device__ __forceinline__ void adj_issue(const AdjDesc<R>& D, int kind, uint32_t tile, unsigned char* stage,
                                           uint32_t fb) {
@@ -436,10 +420,15 @@ __device__ __forceinline__ void adj_issue(const AdjDesc<R>& D, int kind, uint32_
 // kWarpA1: every pass of a warp-local run (A1 in the warp-local layout, strided
 // passes from element bit 9); its own instantiation, so the 12-bit kernel keeps
 // its register allocation.
-template <class R, bool kWarpA1>
+// kW: 0 = the A1 pass; 1..9 = a strided pass of that width (kind TASK_S2 or
+// TASK_S3, whose width the host has matched to kW). One width per instantiation
+// keeps each kernel's code small: a CTA runs only a few tiles per launch, so
+// code that does not fit the instruction cache stalls every warp on fetches.
+template <class R, bool kWarpA1, int kW>
 __global__ void __launch_bounds__(kComputeThreads, 1)
     adj_pass_kernel(const __grid_constant__ AdjDesc<R> D, int kind, uint32_t j, int phase_on, int last_pass,
                     int* err) {
+  static_assert(kW >= 0 && kW <= 9, "strided widths 1..9");
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar;
   __shared__ int is_last;
@@ -452,7 +441,7 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
   const uint32_t fb = smem_addr(&full_bar);
   const uint32_t ntiles = kind == TASK_A1 ? D.n_a1 : (kind == TASK_S2 ? D.n_s2 : D.n_s3);
   const uint32_t part0 = kind == TASK_A1 ? 0u : (kind == TASK_S2 ? D.n_a1 : D.n_a1 + D.n_s2);
-  const int w = kind == TASK_S2 ? D.w2 : D.w3;
+  constexpr int w = kW;
   constexpr int kA1Bits = kWarpA1 ? kA1WarpBits : kElemBits;  // element bits of the step's A1 pass
   const uint32_t h0 = kind == TASK_S2 ? (uint32_t)kA1Bits : (uint32_t)(kA1Bits + D.w2);
   const int mb = kind == TASK_S2 ? D.s2_mid_bits : D.s3_mid_bits;
@@ -477,18 +466,17 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
       if (tid == 0 && nxt < ntiles) adj_issue<R, kWarpA1>(D, kind, nxt, stage, fb);
     };
     double acc;
-    if (kWarpA1 && kind == TASK_A1) {
+    if constexpr (kW == 0 && kWarpA1) {
       acc = adj_a1_warp<R>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
                            phase_on != 0, phase_smem, stage_free);
-    } else if (!kWarpA1 && kind == TASK_A1) {
+    } else if constexpr (kW == 0) {
       acc = adj_a1<R>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
                       phase_on != 0, phase_smem, stage_free);
     } else {
       const uint32_t cp = (uint32_t)(kElemBits - w);
       const uint32_t mid = tile & ((1u << mb) - 1u), hi = tile >> mb;
       const uint32_t tile_base = (mid << cp) | (hi << (h0 + (uint32_t)w));
-      acc = adj_s_dispatch<R>(w, stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, D, tile_base, h0, j, m0,
-                              stage_free);
+      acc = adj_s<R, kW>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, D, tile_base, h0, j, m0, stage_free);
     }
     acc = warp_sum(acc);
     if (lane == 0) red[warp] = acc;

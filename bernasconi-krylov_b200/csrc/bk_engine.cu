@@ -7,6 +7,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <utility>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -1554,6 +1555,20 @@ int evolve_plain(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
 // ---------------------------------------------------------------------------
 constexpr int kResetGrid = 148 * 4;
 
+// the reverse-pass kernel for a pass kind: width 0 = the A1 pass, 1..9 = a strided pass
+template <class R>
+using AdjKernel = void (*)(AdjDesc<R>, int, uint32_t, int, int, int*);
+template <class R, bool kWarpA1, int... W>
+AdjKernel<R> adj_kernel_of(int w, std::integer_sequence<int, W...>) {
+  static const AdjKernel<R> table[] = {adj_pass_kernel<R, kWarpA1, W>...};
+  return table[w];
+}
+template <class R>
+AdjKernel<R> adj_kernel(bool warp_a1, int w) {
+  using Ws = std::make_integer_sequence<int, 10>;
+  return warp_a1 ? adj_kernel_of<R, true>(w, Ws{}) : adj_kernel_of<R, false>(w, Ws{});
+}
+
 // Forward run with checkpoints every K steps (persistent engine), lambda_T = W
 // psi_T, then the reverse sweep: per reverse step one dual A1 / S2 / S3 launch
 // each, a checkpoint put back every K steps. grad_step[k] = dO/dg_k.
@@ -1782,8 +1797,11 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   BK_CUDA(c, cudaMemcpyAsync(base + o_sc, sc_rev.data(), (size_t)T * sizeof(R), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemcpyAsync(base + o_lg, lg_rev.data(), (size_t)T * sizeof(double), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemsetAsync(base + o_ctr, 0, 64, st));
-  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(adj_pass_kernel<R, false>), AdjSmem::kAlloc));
-  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(adj_pass_kernel<R, true>), AdjSmem::kAlloc));
+  // one kernel per pass kind: the A1 pass and a strided pass of each width used
+  const AdjKernel<R> k_a1 = adj_kernel<R>(adj_warp, 0), k_s2 = adj_kernel<R>(adj_warp, w2),
+                     k_s3 = adj_kernel<R>(adj_warp, w3 > 0 ? w3 : w2);
+  for (AdjKernel<R> k : {k_a1, k_s2, k_s3})
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(k), AdjSmem::kAlloc));
   const int ns = c->num_sms;
   const unsigned g1 = std::min<unsigned>(n_a1, (unsigned)ns), g2 = std::min<unsigned>(n_s2, (unsigned)ns),
                  g3 = std::min<unsigned>(std::max<unsigned>(n_s3, 1u), (unsigned)ns);
@@ -1802,29 +1820,16 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   for (int j = 0; j < T; ++j) {
     size_t e = 0;
     BK_TRY(ev_begin(c, "adj_a1", &e));
-    if (adj_warp)
-      adj_pass_kernel<R, true><<<g1, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0,
-                                                                            err);
-    else
-      adj_pass_kernel<R, false><<<g1, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0,
-                                                                             err);
+    k_a1<<<g1, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0, err);
     BK_CUDA(c, cudaGetLastError());
     BK_TRY(ev_end(c, e));
     BK_TRY(ev_begin(c, "adj_s2", &e));
-    if (adj_warp)
-      adj_pass_kernel<R, true><<<g2, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1,
-                                                                            err);
-    else
-      adj_pass_kernel<R, false><<<g2, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S2, (uint32_t)j, 0,
-                                                                             w3 > 0 ? 0 : 1, err);
+    k_s2<<<g2, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1, err);
     BK_CUDA(c, cudaGetLastError());
     BK_TRY(ev_end(c, e));
     if (w3 > 0) {
       BK_TRY(ev_begin(c, "adj_s3", &e));
-      if (adj_warp)
-        adj_pass_kernel<R, true><<<g3, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
-      else
-        adj_pass_kernel<R, false><<<g3, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
+      k_s3<<<g3, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
       BK_CUDA(c, cudaGetLastError());
       BK_TRY(ev_end(c, e));
     }

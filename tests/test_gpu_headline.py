@@ -10,7 +10,7 @@ tests/test_gpu_parity.py::test_golden_series_c128.
 
 Bars (complex64 against complex128), written here:
   * |dP_<| <= C64_DP_BAR (1e-6) at every measured step;
-  * |d<d_H>| <= C64_DH_BAR (3e-6) at every measured step (the reason is written
+  * |d<d_H>| <= C64_DH_BAR (1.2e-5) at every measured step (the reason is written
     beside the constants in tests/conftest.py);
   * state infidelity 1 - |<psi_64|psi_128>|^2 <= 1e-8 at the end of the run.
 """
