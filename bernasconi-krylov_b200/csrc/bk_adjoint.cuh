@@ -68,7 +68,32 @@ struct AdjSmem {
   static constexpr int kRedOff = kPhaseOff + 3328;
   static constexpr int kBytes = kRedOff + 256;
   static constexpr int kAlloc = kBytes + 1024;  // + room to align the stage to 1024 bytes (swizzled TMA)
+  // complex64 A1 with the full phase table (BK_OPT_PHASE_TABLE): a larger phase room
+  static constexpr int kRedOffTab = kPhaseOff + kPhaseTabBytes;
+  static constexpr int kAllocTab = kRedOffTab + 256 + 1024;
 };
+
+// D^dagger on the same element of psi (v) and lambda (u): one set of rotation
+// coefficients for both; kTab (complex64): from the full phase table, the two
+// half-angle shear rotations negated (a shear triple with (-a, -b) undoes (a, b))
+template <class R, bool kTab>
+__device__ __forceinline__ void adj_phase_inv(typename El<R>::T& v, typename El<R>::T& u, uint32_t e,
+                                              const typename PhaseV<R>::params& P, const unsigned char* phase_smem) {
+  if constexpr (kTab) {
+    const float2* tab = reinterpret_cast<const float2*>(phase_smem);
+    const uint32_t c0 = (uint32_t)P.c0;
+    const float2 H0 = tab[((e & 0xFFFFu) - c0) >> 2], H1 = tab[((e >> 16) - c0) >> 2];
+    const float2 A = make_float2(-H0.x, -H1.x), B = make_float2(-H0.y, -H1.y);
+    PhaseV<float>::shear2(v.re, v.im, A, B);
+    PhaseV<float>::shear2(v.re, v.im, A, B);
+    PhaseV<float>::shear2(u.re, u.im, A, B);
+    PhaseV<float>::shear2(u.re, u.im, A, B);
+  } else {
+    const typename PhaseV<R>::Coef cf = PhaseV<R>::coef(e, P, phase_smem, true);
+    PhaseV<R>::rotate(v, cf, true);
+    PhaseV<R>::rotate(u, cf, true);
+  }
+}
 
 __host__ __device__ constexpr int popc_c(uint32_t x) { return x ? (int)(x & 1u) + popc_c(x >> 1) : 0; }
 
@@ -147,7 +172,7 @@ __device__ __forceinline__ double round_weight(int m, double lg1t2) { return exp
 
 // reverse A1 on a staged (psi, lambda, E) tile: D^dagger, rescale, low-qubit
 // butterflies with their cross terms. Returns this thread's weighted sum.
-template <class R, class F>
+template <class R, bool kTab, class F>
 __device__ __forceinline__ double adj_a1(unsigned char* sp, unsigned char* sl, const unsigned char* etile,
                                          const AdjDesc<R>& D, uint32_t t_idx, uint32_t j, bool phase_on,
                                          const unsigned char* phase_smem, F&& stage_free) {
@@ -168,11 +193,8 @@ __device__ __forceinline__ double adj_a1(unsigned char* sp, unsigned char* sl, c
 #pragma unroll
   for (int q = 0; q < 16; ++q) {
     if (phase_on) {
-      // one set of rotation coefficients for both statevectors
       const uint32_t e = load_e<R>(etile, b1 | pdep((uint32_t)q, PL::A1_R1_REG));
-      const typename PhaseV<R>::Coef cf = PhaseV<R>::coef(e, D.phase, phase_smem, true);
-      PhaseV<R>::rotate(v[q], cf, true);
-      PhaseV<R>::rotate(u[q], cf, true);
+      adj_phase_inv<R, kTab>(v[q], u[q], e, D.phase, phase_smem);
     }
     if (sc != (R)1) {
       E::scale(v[q], sc);
@@ -229,7 +251,7 @@ __device__ __forceinline__ double adj_a1(unsigned char* sp, unsigned char* sl, c
 // rescale, amplitude bit 0, round 1 (register bits 0-2, 6) and round 2
 // (register bits 3-5, 7) with their cross terms, bit 8 across lanes 16 apart.
 // The only CTA barrier releases the stage after round 2's reads.
-template <class R, class F>
+template <class R, bool kTab, class F>
 __device__ __forceinline__ double adj_a1_warp(unsigned char* sp, unsigned char* sl, const unsigned char* etile,
                                               const AdjDesc<R>& D, uint32_t t_idx, uint32_t j, bool phase_on,
                                               const unsigned char* phase_smem, F&& stage_free) {
@@ -259,10 +281,7 @@ __device__ __forceinline__ double adj_a1_warp(unsigned char* sp, unsigned char* 
       load_e8<R>(etile, b1 | ((uint32_t)h << 6), ev);
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        // one set of rotation coefficients for both statevectors
-        const typename PhaseV<R>::Coef cf = PhaseV<R>::coef(ev[q], D.phase, phase_smem, true);
-        PhaseV<R>::rotate(v[8 * h + q], cf, true);
-        PhaseV<R>::rotate(u[8 * h + q], cf, true);
+        adj_phase_inv<R, kTab>(v[8 * h + q], u[8 * h + q], ev[q], D.phase, phase_smem);
       }
     }
   }
@@ -424,11 +443,12 @@ __device__ __forceinline__ void adj_issue(const AdjDesc<R>& D, int kind, uint32_
 // TASK_S3, whose width the host has matched to kW). One width per instantiation
 // keeps each kernel's code small: a CTA runs only a few tiles per launch, so
 // code that does not fit the instruction cache stalls every warp on fetches.
-template <class R, bool kWarpA1, int kW>
+template <class R, bool kWarpA1, int kW, bool kTab = false>
 __global__ void __launch_bounds__(kComputeThreads, 1)
     adj_pass_kernel(const __grid_constant__ AdjDesc<R> D, int kind, uint32_t j, int phase_on, int last_pass,
                     int* err) {
   static_assert(kW >= 0 && kW <= 9, "strided widths 1..9");
+  static_assert(!kTab || (kW == 0 && sizeof(R) == 4), "the full phase table: complex64 A1 passes only");
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar;
   __shared__ int is_last;
@@ -436,7 +456,7 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
   unsigned char* smem = kWarpA1 ? smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u) : smem_raw;
   unsigned char* stage = smem;
   unsigned char* phase_smem = smem + AdjSmem::kPhaseOff;
-  double* red = reinterpret_cast<double*>(smem + AdjSmem::kRedOff);
+  double* red = reinterpret_cast<double*>(smem + (kTab ? AdjSmem::kRedOffTab : AdjSmem::kRedOff));
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t fb = smem_addr(&full_bar);
   const uint32_t ntiles = kind == TASK_A1 ? D.n_a1 : (kind == TASK_S2 ? D.n_s2 : D.n_s3);
@@ -448,13 +468,24 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
   // qubits rotated by the earlier passes of the step (complex64: + amplitude bit 0)
   const int m0 = (sizeof(R) == 4 ? 1 : 0) + kA1Bits + (kind == TASK_S3 ? D.w2 : 0);
   uint32_t tile = blockIdx.x;
-  // the first tile's loads go out before the phase tables are staged
+  // Launched as a programmatic dependent of the previous pass: the barrier and
+  // the phase tables (constant over the sweep) are set up while that pass
+  // finishes; everything the previous passes write (psi, lambda, the step's
+  // partials and ticket) is touched only after the grid-dependency wait.
   if (tid == 0) {
     mbar_init(fb, 1);
     fence_barrier_init();
-    if (tile < ntiles) adj_issue<R, kWarpA1>(D, kind, tile, stage, fb);
   }
-  if (kind == TASK_A1 && phase_on) PhaseV<R>::stage(D.phase, phase_smem, tid, kComputeThreads);
+  if (kind == TASK_A1 && phase_on) {
+    if constexpr (kTab) {
+      float2* tab = reinterpret_cast<float2*>(phase_smem);
+      for (int i = tid; i < D.phase.n_j; i += kComputeThreads) tab[i] = D.phase.tab[i];
+    } else {
+      PhaseV<R>::stage(D.phase, phase_smem, tid, kComputeThreads);
+    }
+  }
+  grid_dependency_wait();
+  if (tid == 0 && tile < ntiles) adj_issue<R, kWarpA1>(D, kind, tile, stage, fb);
   __syncthreads();
   uint32_t parity = 0;
   for (; tile < ntiles; tile += gridDim.x) {
@@ -462,15 +493,17 @@ __global__ void __launch_bounds__(kComputeThreads, 1)
     if (__syncthreads_or(!ok)) return;
     parity ^= 1u;
     const uint32_t nxt = tile + gridDim.x;
+    // the CTA's last tile: the next pass may be scheduled onto SMs as they free up
+    if (nxt >= ntiles) grid_dependents_launch();
     auto stage_free = [&]() {
       if (tid == 0 && nxt < ntiles) adj_issue<R, kWarpA1>(D, kind, nxt, stage, fb);
     };
     double acc;
     if constexpr (kW == 0 && kWarpA1) {
-      acc = adj_a1_warp<R>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
+      acc = adj_a1_warp<R, kTab>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
                            phase_on != 0, phase_smem, stage_free);
     } else if constexpr (kW == 0) {
-      acc = adj_a1<R>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
+      acc = adj_a1<R, kTab>(stage + AdjSmem::kPsiOff, stage + AdjSmem::kLamOff, stage + AdjSmem::kEOff, D, tile, j,
                       phase_on != 0, phase_smem, stage_free);
     } else {
       const uint32_t cp = (uint32_t)(kElemBits - w);

@@ -1555,6 +1555,25 @@ int evolve_plain(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, double
 // ---------------------------------------------------------------------------
 constexpr int kResetGrid = 148 * 4;
 
+// A launch that may start while the previous kernel on the stream finishes
+// (programmatic dependent launch): the kernel itself waits (griddepcontrol.wait)
+// before it touches anything that kernel writes.
+template <class... P, class... A>
+cudaError_t launch_dependent(void (*kern)(P...), unsigned grid, unsigned block, int smem, cudaStream_t st,
+                             A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
 // the reverse-pass kernel for a pass kind: width 0 = the A1 pass, 1..9 = a strided pass
 template <class R>
 using AdjKernel = void (*)(AdjDesc<R>, int, uint32_t, int, int, int*);
@@ -1567,6 +1586,14 @@ template <class R>
 AdjKernel<R> adj_kernel(bool warp_a1, int w) {
   using Ws = std::make_integer_sequence<int, 10>;
   return warp_a1 ? adj_kernel_of<R, true>(w, Ws{}) : adj_kernel_of<R, false>(w, Ws{});
+}
+// the reverse A1 pass with the full complex64 phase table (complex128 has none)
+template <class R>
+AdjKernel<R> adj_table_kernel(bool warp_a1) {
+  if constexpr (sizeof(R) == 4)
+    return warp_a1 ? adj_pass_kernel<R, true, 0, true> : adj_pass_kernel<R, false, 0, true>;
+  else
+    return adj_kernel<R>(warp_a1, 0);
 }
 
 // Forward run with checkpoints every K steps (persistent engine), lambda_T = W
@@ -1734,6 +1761,12 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   const size_t o_ctr = b.take(64);
   const size_t o_cross = b.take((size_t)T * sizeof(double));
   const size_t o_dev = b.take(std::max<size_t>(resets.size(), 1) * kResetGrid * sizeof(double));
+  // complex64 reverse A1 with the full phase table (BK_OPT_PHASE_TABLE)
+  std::vector<float2> ptab;
+  typename PhaseV<R>::params aph = run.phase;
+  if constexpr (kC64)
+    if (c->phase_table) BK_TRY(build_phase_table(c, n, angle_unit, &aph, &ptab));
+  const size_t o_ptab = b.take(std::max<size_t>(ptab.size(), 1) * sizeof(float2));
   BK_TRY(ensure_buffer(c, &c->d_adj, &c->adj_cap, b.off));
   char* base = static_cast<char*>(c->d_adj);
   CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(base + o_maps);
@@ -1781,7 +1814,9 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   A.s3_mid_dim = w3 > 0 ? s3p.mid_dim : -1;
   A.s3_hi_dim = w3 > 0 ? s3p.hi_dim : -1;
   A.s3_mid_bits = w3 > 0 ? (int)s3p.mid_bits : 0;
-  A.phase = run.phase;
+  if constexpr (kC64)
+    if (!ptab.empty()) aph.tab = reinterpret_cast<const float2*>(base + o_ptab);
+  A.phase = aph;
   A.tan = reinterpret_cast<const R*>(base + o_tan);
   A.scale = reinterpret_cast<const R*>(base + o_sc);
   A.lg1t2 = reinterpret_cast<const double*>(base + o_lg);
@@ -1798,10 +1833,15 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   BK_CUDA(c, cudaMemcpyAsync(base + o_lg, lg_rev.data(), (size_t)T * sizeof(double), cudaMemcpyHostToDevice, st));
   BK_CUDA(c, cudaMemsetAsync(base + o_ctr, 0, 64, st));
   // one kernel per pass kind: the A1 pass and a strided pass of each width used
-  const AdjKernel<R> k_a1 = adj_kernel<R>(adj_warp, 0), k_s2 = adj_kernel<R>(adj_warp, w2),
+  if (!ptab.empty())
+    BK_CUDA(c, cudaMemcpyAsync(base + o_ptab, ptab.data(), ptab.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
+  const bool a_tab = !ptab.empty();
+  const int a1_smem = a_tab ? AdjSmem::kAllocTab : AdjSmem::kAlloc;
+  const AdjKernel<R> k_a1 = a_tab ? adj_table_kernel<R>(adj_warp) : adj_kernel<R>(adj_warp, 0),
+                     k_s2 = adj_kernel<R>(adj_warp, w2),
                      k_s3 = adj_kernel<R>(adj_warp, w3 > 0 ? w3 : w2);
   for (AdjKernel<R> k : {k_a1, k_s2, k_s3})
-    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(k), AdjSmem::kAlloc));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(k), k == k_a1 ? a1_smem : AdjSmem::kAlloc));
   const int ns = c->num_sms;
   const unsigned g1 = std::min<unsigned>(n_a1, (unsigned)ns), g2 = std::min<unsigned>(n_s2, (unsigned)ns),
                  g3 = std::min<unsigned>(std::max<unsigned>(n_s3, 1u), (unsigned)ns);
@@ -1820,17 +1860,17 @@ int adjoint_t(bk_ctx* c, const bk_adjoint_params* p, const std::vector<double>& 
   for (int j = 0; j < T; ++j) {
     size_t e = 0;
     BK_TRY(ev_begin(c, "adj_a1", &e));
-    k_a1<<<g1, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_A1, (uint32_t)j, j > 0 ? 1 : 0, 0, err);
-    BK_CUDA(c, cudaGetLastError());
+    BK_CUDA(c, launch_dependent(k_a1, g1, kComputeThreads, a1_smem, st, A, (int)TASK_A1, (uint32_t)j, j > 0 ? 1 : 0,
+                                0, err));
     BK_TRY(ev_end(c, e));
     BK_TRY(ev_begin(c, "adj_s2", &e));
-    k_s2<<<g2, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S2, (uint32_t)j, 0, w3 > 0 ? 0 : 1, err);
-    BK_CUDA(c, cudaGetLastError());
+    BK_CUDA(c, launch_dependent(k_s2, g2, kComputeThreads, AdjSmem::kAlloc, st, A, (int)TASK_S2, (uint32_t)j, 0,
+                                w3 > 0 ? 0 : 1, err));
     BK_TRY(ev_end(c, e));
     if (w3 > 0) {
       BK_TRY(ev_begin(c, "adj_s3", &e));
-      k_s3<<<g3, kComputeThreads, AdjSmem::kAlloc, st>>>(A, TASK_S3, (uint32_t)j, 0, 1, err);
-      BK_CUDA(c, cudaGetLastError());
+      BK_CUDA(c, launch_dependent(k_s3, g3, kComputeThreads, AdjSmem::kAlloc, st, A, (int)TASK_S3, (uint32_t)j, 0,
+                                  1, err));
       BK_TRY(ev_end(c, e));
     }
     if (ri < resets.size() && resets[ri].after_j == j) {

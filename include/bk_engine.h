@@ -302,8 +302,9 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       A1 kernels 1-3: 1 = the diagonal phase of every energy level from one
  *       table entry (E = floor(n/2) mod 4 for every LABS energy, so at most 2139
  *       levels, 17 KB) applied as two half-angle shear rotations; 0 (default) =
- *       a 16-entry level table and residual polynomials. Other kernels and
- *       complex128 ignore it. */
+ *       a 16-entry level table and residual polynomials. bk_adjoint's complex64
+ *       reverse A1 pass takes it too (D^dagger as the negated rotations); other
+ *       kernels and complex128 ignore it. */
 enum {
   BK_OPT_ENGINE_MODE = 0,
   BK_OPT_SLAB_LAG = 1,

@@ -61,6 +61,28 @@ def test_adjoint_c64_matches_oracle(eng, n):
     assert st["max_drift"] <= 1e-4
 
 
+@pytest.mark.parametrize("n,adj_a1", [(18, 0), (22, 0), (23, 0), (22, 1)])
+def test_adjoint_c64_phase_table_matches_oracle(eng, n, adj_a1):
+    """The reverse A1 pass with the full complex64 phase table (BK_OPT_PHASE_TABLE:
+    D^dagger as the negated half-angle shear rotations of each level's entry), in
+    the 12-bit and the warp-local layouts: the same bars as the level-table path."""
+    T, K = (24, 8) if n >= 22 else (40, 16)
+    bits, e0, gs, seg = _case(n, 4, T, n)
+    eng.set_option("phase_table", 1)
+    eng.set_option("adj_a1", adj_a1)
+    try:
+        val, grad, st = eng.adjoint(n, bits, gs, 0.05, T, e0=e0, precision=bk.BK_C64, checkpoint_every=K,
+                                    per_step=True)
+    finally:
+        eng.set_option("phase_table", 0)
+        eng.set_option("adj_a1", 0)
+    oval, ograd = O.trotter_adjoint(n, bits, e0, gs[seg], 0.05, T)
+    scale = np.max(np.abs(ograd))
+    assert abs(val - oval) <= 1e-6
+    assert np.max(np.abs(st["grad_steps"] - ograd)) <= 1e-4 * scale
+    assert st["max_drift"] <= 1e-4
+
+
 def test_adjoint_d_h_objective_c128(eng):
     n, T = 16, 36
     bits, e0, gs, seg = _case(n, 6, T, 5)
