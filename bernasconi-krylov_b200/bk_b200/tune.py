@@ -16,7 +16,7 @@ Knobs (engine options, include/bk_engine.h):
                0-8 inside each warp, no CTA barrier; the strided passes take
                bits 9 and up; up to 27 element bits), 3 = warp-local with
                4-warp CTAs over 32 KB half tiles (four CTAs per SM);
-  phase_table  complex64 per-pass A1 kernels 1-3: 1 = the diagonal phase of
+  phase_table  complex64 per-pass A1 kernels: 1 = the diagonal phase of
                each energy level from a full table (E = floor(n/2) mod 4 for
                every LABS energy) as two half-angle shear rotations, 0 = level
                table and residual polynomials.
@@ -93,7 +93,7 @@ def candidates(n, precision):
         fused(rest9, [0] + [w for w in (d9 - 1, d9 + 1) if 3 <= w <= 9 and w <= rest9 and rest9 - w <= 9], (2, 3))
     # complex64: the full phase table with every per-pass candidate whose A1 kernel takes it (1-3)
     if precision == BK_C64:
-        out += [dict(c, phase_table=1) for c in list(out) if c["engine_mode"] in (1, 2) and c["a1_wide"] >= 1]
+        out += [dict(c, phase_table=1) for c in list(out) if c["engine_mode"] in (1, 2)]
     # E recomputed in the pass, on the default split of both schedules
     out.append(dict(engine_mode=1, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))
     out.append(dict(engine_mode=0, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))

@@ -652,6 +652,7 @@ template <class R>
 int allow_table_a1(bk_ctx* c) {
   if constexpr (sizeof(R) == 4) {
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_wide_kernel<R, true>), A1Smem<true>::kBytes));
+    BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_tab_kernel<R>), A1Smem<true>::kBytes));
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 8, true>), WarpA1Smem<8, true>::kBytes));
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(tile_a1_warp_kernel<R, 4, true>), WarpA1Smem<4, true>::kBytes));
   }
@@ -664,8 +665,10 @@ void launch_table_a1(const InstDesc<R>& D, int a1_wide, uint32_t n_a1, cudaStrea
       tile_a1_warp_kernel<R, 4, true><<<2 * n_a1, 128, WarpA1Smem<4, true>::kBytes, st>>>(D, step, err);
     else if (D.a1_bits == kA1WarpBits)
       tile_a1_warp_kernel<R, 8, true><<<n_a1, kComputeThreads, WarpA1Smem<8, true>::kBytes, st>>>(D, step, err);
-    else
+    else if (a1_wide == 1)
       tile_a1_wide_kernel<R, true><<<n_a1, kA1WideThreads, A1Smem<true>::kBytes, st>>>(D, step, err);
+    else
+      tile_a1_tab_kernel<R><<<n_a1, kComputeThreads, A1Smem<true>::kBytes, st>>>(D, step, err);
   }
 }
 
@@ -707,8 +710,8 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   std::vector<float2> ptab;
   if constexpr (sizeof(R) == 4) {
     BK_TRY(build_phase_v(c, n, angle_unit, &ph, &hab));
-    // the full phase table for the per-pass 512-thread and warp-local A1 kernels
-    if (grid_mode && c->phase_table && (c->a1_wide == 1 || a1_warp))
+    // the full phase table for the per-pass A1 kernels
+    if (grid_mode && c->phase_table)
       BK_TRY(build_phase_table(c, n, angle_unit, &ph, &ptab));
   } else {
     Phase64 p64{};

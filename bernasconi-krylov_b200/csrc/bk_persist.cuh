@@ -472,11 +472,49 @@ __device__ __forceinline__ void compute_reduce(MeasureAcc acc, double* partials,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Full phase table (BK_OPT_PHASE_TABLE, complex64 per-pass A1 kernels): every
+// LABS energy is E = c0 + 4 j with c0 = floor(n/2) mod 4, so one table entry
+// {-tan(r/4), sin(r/2)} per level j (r = theta E reduced to (-pi, pi]) gives the
+// rotation as two half-angle shear rotations: no level split and no residual
+// polynomial, a third of the phase's FMA work. The table (at most 2139 entries,
+// 17 KB at n = 30) arrives by one bulk copy on the tile's own barrier.
+// ---------------------------------------------------------------------------
+constexpr int kPhaseTabMax = 2144;  // >= (8555 - 3) / 4 + 1 entries at n = 30, even
+constexpr int kPhaseTabBytes = kPhaseTabMax * (int)sizeof(float2);
+static_assert(kPhaseTabBytes >= 3328, "the table room also holds the level tables");
+
+// bytes of the table copy (the count rounded up to an even number of entries: 16-byte multiple)
+__device__ __forceinline__ uint32_t phase_tab_bytes(const PhaseV32& P) {
+  return (uint32_t)((P.n_j + 1) & ~1) * (uint32_t)sizeof(float2);
+}
+
+// the full-table rotation of a complex64 element (two amplitudes, energies packed in e2)
+__device__ __forceinline__ void phase_table_apply(El<float>::T& v, uint32_t e2, const unsigned char* s,
+                                                  uint32_t c0) {
+  const float2* tab = reinterpret_cast<const float2*>(s);
+  const uint32_t j0 = ((e2 & 0xFFFFu) - c0) >> 2, j1 = ((e2 >> 16) - c0) >> 2;
+  const float2 H0 = tab[j0], H1 = tab[j1];
+  const float2 A = make_float2(H0.x, H1.x), B = make_float2(H0.y, H1.y);
+  PhaseV<float>::shear2(v.re, v.im, A, B);
+  PhaseV<float>::shear2(v.re, v.im, A, B);
+}
+
+// the A1 kernels' phase: the full table (kTab, complex64) or the level table with residual polynomials
+template <class R, bool kTab>
+__device__ __forceinline__ void a1_phase(typename El<R>::T& v, uint32_t e, const InstDesc<R>& D,
+                                         const unsigned char* phase_smem) {
+  if constexpr (kTab)
+    phase_table_apply(v, e, phase_smem, (uint32_t)D.phase.c0);
+  else
+    PhaseV<R>::apply(v, e, D.phase, phase_smem, false);
+}
+
 // A1 (and measurement-only M) on a staged tile
 // `stage_free()` runs (in every thread, after a barrier) as soon as the last
 // shared-memory read of the staged tile is done, so the next tile's load can be
 // issued while this tile's last round computes and its stores drain.
-template <class R, bool MEASURE_ONLY, class F>
+template <class R, bool MEASURE_ONLY, bool kTab = false, class F>
 __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned char* etile, const InstDesc<R>& D,
                                            uint32_t t_idx, uint32_t step, const unsigned char* phase_smem,
                                            double* red, int* last_flag, F&& stage_free) {
@@ -509,7 +547,7 @@ __device__ __forceinline__ void process_a1(unsigned char* tile, const unsigned c
     const uint32_t e = D.e_recompute ? recompute_e<R>(tile_base | i, D.n) : load_e<R>(etile, i);
     if (slot >= 0) measure_el(acc, v[j], e, tile_base | i, D.e0, D.s0);
     if (!MEASURE_ONLY) {
-      PhaseV<R>::apply(v[j], e, D.phase, phase_smem, false);
+      a1_phase<R, kTab>(v[j], e, D, phase_smem);
       E::bfly_inner(v[j], t);
     }
   }
@@ -858,44 +896,6 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
   if (tid == 0 && inflight) mbar_wait_bounded(fb, phase, P.err);
 }
 
-// ---------------------------------------------------------------------------
-// Full phase table (BK_OPT_PHASE_TABLE, complex64 per-pass A1 kernels): every
-// LABS energy is E = c0 + 4 j with c0 = floor(n/2) mod 4, so one table entry
-// {-tan(r/4), sin(r/2)} per level j (r = theta E reduced to (-pi, pi]) gives the
-// rotation as two half-angle shear rotations: no level split and no residual
-// polynomial, a third of the phase's FMA work. The table (at most 2139 entries,
-// 17 KB at n = 30) arrives by one bulk copy on the tile's own barrier.
-// ---------------------------------------------------------------------------
-constexpr int kPhaseTabMax = 2144;  // >= (8555 - 3) / 4 + 1 entries at n = 30, even
-constexpr int kPhaseTabBytes = kPhaseTabMax * (int)sizeof(float2);
-static_assert(kPhaseTabBytes >= 3328, "the table room also holds the level tables");
-
-// bytes of the table copy (the count rounded up to an even number of entries: 16-byte multiple)
-__device__ __forceinline__ uint32_t phase_tab_bytes(const PhaseV32& P) {
-  return (uint32_t)((P.n_j + 1) & ~1) * (uint32_t)sizeof(float2);
-}
-
-// the full-table rotation of a complex64 element (two amplitudes, energies packed in e2)
-__device__ __forceinline__ void phase_table_apply(El<float>::T& v, uint32_t e2, const unsigned char* s,
-                                                  uint32_t c0) {
-  const float2* tab = reinterpret_cast<const float2*>(s);
-  const uint32_t j0 = ((e2 & 0xFFFFu) - c0) >> 2, j1 = ((e2 >> 16) - c0) >> 2;
-  const float2 H0 = tab[j0], H1 = tab[j1];
-  const float2 A = make_float2(H0.x, H1.x), B = make_float2(H0.y, H1.y);
-  PhaseV<float>::shear2(v.re, v.im, A, B);
-  PhaseV<float>::shear2(v.re, v.im, A, B);
-}
-
-// the A1 kernels' phase: the full table (kTab, complex64) or the level table with residual polynomials
-template <class R, bool kTab>
-__device__ __forceinline__ void a1_phase(typename El<R>::T& v, uint32_t e, const InstDesc<R>& D,
-                                         const unsigned char* phase_smem) {
-  if constexpr (kTab)
-    phase_table_apply(v, e, phase_smem, (uint32_t)D.phase.c0);
-  else
-    PhaseV<R>::apply(v, e, D.phase, phase_smem, false);
-}
-
 // shared memory of a 64 KB-tile A1 kernel: the stage, the phase room, reduction scratch
 template <bool kTab>
 struct A1Smem {
@@ -1074,6 +1074,41 @@ __global__ void __launch_bounds__(kComputeThreads, 2)
     const uint32_t tile_base = (mid << cp) | (hi << (h0 + (uint32_t)w));
     process_s_dispatch<R>(w, stage, D.state, tile_base, h0, D.tan[step], none);
   }
+}
+
+// The 256-thread A1 (BK_OPT_A1_WIDE = 0) as its own grid kernel with the full
+// phase table (complex64): three rounds of 16 elements per thread move each
+// element through shared memory five times against seven in the 512-thread A1,
+// which matters once the table's lookups share the shared-memory pipe.
+template <class R>
+__global__ void __launch_bounds__(kComputeThreads, 2)
+    tile_a1_tab_kernel(const __grid_constant__ InstDesc<R> D, uint32_t step, int* err) {
+  static_assert(sizeof(R) == 4, "the full phase table is complex64 only");
+  using SM = A1Smem<true>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full_bar;
+  __shared__ int last_flag;
+  unsigned char* stage = smem;
+  unsigned char* phase_smem = smem + SM::kPhaseOff;
+  double* red = reinterpret_cast<double*>(smem + SM::kRedOff);
+  const uint32_t fb = smem_addr(&full_bar);
+  StageMeta m;
+  m.kind = TASK_A1;
+  m.inst = 0;
+  m.tile = blockIdx.x;
+  m.step = step;
+  if (threadIdx.x == 0) {
+    mbar_init(fb, 1);
+    fence_barrier_init();
+    const uint32_t tb = phase_tab_bytes(D.phase);
+    issue_task_load(D, m, stage, fb, tb);
+    bulk_load(smem_addr(phase_smem), D.phase.tab, tb, fb);
+  }
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(fb, 0, err);
+  if (__syncthreads_or(!ok)) return;
+  auto none = []() {};
+  process_a1<R, false, true>(stage, stage + kStageTileBytes, D, m.tile, step, phase_smem, red, &last_flag, none);
 }
 
 // ---------------------------------------------------------------------------

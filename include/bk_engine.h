@@ -298,8 +298,8 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       launch wait for one completion more than can arrive, as if a producer
  *       were lost; the bounded wait runs out, every CTA leaves, and bk_evolve
  *       returns BK_ERR_TIMEOUT with the context still usable;
- *   BK_OPT_PHASE_TABLE: complex64, per-pass schedules (modes 1 and 2) with the
- *       A1 kernels 1-3: 1 = the diagonal phase of every energy level from one
+ *   BK_OPT_PHASE_TABLE: complex64, per-pass schedules (modes 1 and 2), every
+ *       A1 kernel: 1 = the diagonal phase of every energy level from one
  *       table entry (E = floor(n/2) mod 4 for every LABS energy, so at most 2139
  *       levels, 17 KB) applied as two half-angle shear rotations; 0 (default) =
  *       a 16-entry level table and residual polynomials. bk_adjoint's complex64

@@ -40,7 +40,7 @@ def _run(eng, n, bits, e0, steps, every, precision, mode, a1, table, g=0.35, dt=
 
 
 @pytest.mark.parametrize("mode", [1, 2])
-@pytest.mark.parametrize("a1", [1, 2, 3])
+@pytest.mark.parametrize("a1", [0, 1, 2, 3])
 def test_phase_table_matches_oracle(eng, mode, a1):
     """complex64 with the full table, every A1 kernel that takes it, both
     per-pass schedules: within the complex64 bars of the complex128 oracle."""
@@ -64,11 +64,11 @@ def test_phase_table_long_run_against_c128(eng):
 
 
 def test_phase_table_ignored_where_unused(eng):
-    """complex128, and the 256-thread A1 (kernel 0), do not take the table: their
-    series are bit-identical with the option on and off."""
-    for n, prec, a1 in ((21, bk.BK_C128, 1), (22, bk.BK_C64, 0)):
+    """complex128 and the persistent schedule (mode 0) do not take the table:
+    their series are bit-identical with the option on and off."""
+    for n, prec, a1, mode in ((21, bk.BK_C128, 1, 1), (22, bk.BK_C64, 0, 0)):
         bits, e0 = bk.select_trap(n, 6, 200, 0.05)
-        off = _run(eng, n, bits, e0, 12, 3, prec, 1, a1, 0)
-        on = _run(eng, n, bits, e0, 12, 3, prec, 1, a1, 1)
+        off = _run(eng, n, bits, e0, 12, 3, prec, mode, a1, 0)
+        on = _run(eng, n, bits, e0, 12, 3, prec, mode, a1, 1)
         for a, b in zip(off, on):
             assert np.array_equal(a, b), (n, prec)
