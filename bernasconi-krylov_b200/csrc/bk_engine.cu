@@ -116,6 +116,8 @@ struct bk_ctx {
   size_t ckpt_cap = 0;
   void* d_adj = nullptr;      // adjoint: maps, descriptor, per-step arrays, partials
   size_t adj_cap = 0;
+  void* d_fsmap = nullptr;    // full-space strided pass: the tensor map of x (device memory, 64-byte aligned)
+  size_t fsmap_cap = 0;
   void* d_descent = nullptr;  // batched steepest descent: starts, final states, energies, evaluations
   size_t descent_cap = 0;
   void* d_lz = nullptr;       // full-space Lanczos: Krylov basis, work vector, partial sums, alpha / beta
@@ -1998,7 +2000,7 @@ int bk_destroy(bk_ctx* c) {
     if (p) cudaFree(p);
   for (auto& kv : c->batch_E) cudaFree(kv.second);
   for (void* p : {c->d_batch_state, c->d_batch, (void*)c->d_batch_results, c->d_persist, c->d_lam, c->d_ckpt,
-                  c->d_adj, c->d_descent, c->d_lz})
+                  c->d_adj, c->d_descent, c->d_lz, c->d_fsmap})
     if (p) cudaFree(p);
   for (auto& e : c->ev_pool) {
     cudaEventDestroy(e.first);
@@ -2856,7 +2858,7 @@ int fs_matvec(bk_ctx* c, int n, double g, double scale, const double* x, double*
   BK_TRY(ensure_energy(c, n));
   const int tile_bytes = (1 << kFsTileBits) * (int)sizeof(double);
   size_t ev = 0;
-  BK_TRY(ev_begin(c, "fs_pass", &ev));
+  BK_TRY(ev_begin(c, n < kFsTileBits ? "fs_pass" : "fs_block", &ev));
   if (n < kFsTileBits) {
     BK_TRY(allow_smem(c, reinterpret_cast<const void*>(fs_pass_kernel), tile_bytes));
     fs_pass_kernel<<<1, kFsThreads, (size_t)(1u << n) * sizeof(double), c->stream>>>(x, y, c->d_E, scale, g, n, n, n,
@@ -2866,7 +2868,7 @@ int fs_matvec(bk_ctx* c, int n, double g, double scale, const double* x, double*
     return BK_OK;
   }
   BK_TRY(allow_smem(c, reinterpret_cast<const void*>(fs_block_kernel), tile_bytes));
-  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(fs_tile_kernel), tile_bytes));
+  BK_TRY(allow_smem(c, reinterpret_cast<const void*>(fs_tile_kernel), kFsTileSmem));
   const uint32_t tiles = 1u << (n - kFsTileBits);
   fs_block_kernel<<<tiles, kFsThreads, tile_bytes, c->stream>>>(x, y, c->d_E, scale, g, std::min(n, kFsGatherBits),
                                                                 c->d_err);
@@ -2874,9 +2876,17 @@ int fs_matvec(bk_ctx* c, int n, double g, double scale, const double* x, double*
   BK_TRY(ev_end(c, ev));
   if (n > kFsGatherBits) {
     const int w = n - kFsGatherBits, cp = kFsTileBits - w, h0 = kFsGatherBits;
-    BK_TRY(ev_begin(c, "fs_pass", &ev));
-    fs_tile_kernel<<<tiles, kFsThreads, tile_bytes, c->stream>>>(x, y, c->d_E, scale, g, cp, h0, h0 - cp, 0, cp,
-                                                                  c->d_err);
+    // x as 2^n doubles (8-byte TMA elements): runs of 2^cp, 2^w of them 2^h0 apart, tiles over bits [cp, h0)
+    TmaDesc xm;
+    BK_TRY(build_amp_map(c, const_cast<double*>(x), n, BK_C64, cp, h0, w, &xm));
+    if (xm.hi_dim >= 0 || (int)xm.mid_bits != h0 - cp)
+      return fail(c, BK_ERR_UNSUPPORTED, "full-space strided pass: tile geometry for n = %d", n);
+    BK_TRY(ensure_buffer(c, &c->d_fsmap, &c->fsmap_cap, sizeof(CUtensorMap)));
+    BK_CUDA(c, cudaMemcpyAsync(c->d_fsmap, &xm.map, sizeof(CUtensorMap), cudaMemcpyHostToDevice, c->stream));
+    BK_TRY(ev_begin(c, "fs_tile", &ev));
+    fs_tile_kernel<<<tiles, kFsThreads, kFsTileSmem, c->stream>>>(static_cast<const CUtensorMap*>(c->d_fsmap), y,
+                                                                   c->d_E, scale, g, cp, h0, h0 - cp,
+                                                                  xm.mid_dim, xm.hi_dim, 0, cp, c->d_err);
     BK_CUDA(c, cudaGetLastError());
     BK_TRY(ev_end(c, ev));
   }

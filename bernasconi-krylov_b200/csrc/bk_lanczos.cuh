@@ -11,14 +11,15 @@
 //     coalesced sweeps of the partner blocks (L2 hits: partners <= 32 MB away),
 //     the diagonal from the cached uint16 E table, y stored streaming;
 //   strided pass (fs_tile_kernel, n > 23): tiles of index bits [0, 13 - w) u
-//     [23, n), w = n - 23 <= 7 (runs of >= 64 doubles), y -= g sum x[i ^ 2^j]
-//     for the far bits with every partner inside the tile.
+//     [23, n), w = n - 23 <= 7 (runs of >= 64 doubles) loaded as one tensor-map
+//     box, y -= g sum x[i ^ 2^j] for the far bits with every partner inside the tile.
 // DRAM per state: x, E, y once (18 B) plus x, y, y (24 B) for the far bits.
 //
 // Lanczos steps (the driver's cuBLAS calls, :437-482) are fused element-wise
 // kernels with per-block partial sums reduced in a fixed order (deterministic).
 #pragma once
 #include "bk_device.cuh"
+#include "bk_fused.cuh"
 
 namespace bk {
 
@@ -53,33 +54,46 @@ __global__ void __launch_bounds__(kFsThreads) fs_pass_kernel(const double* __res
 
 
 constexpr int kFsPer = (1 << kFsTileBits) / kFsThreads;  // 32 tile positions per thread
+constexpr int kFsTileSmem = (1 << kFsTileBits) * (int)sizeof(double) + 128;  // strided pass: tile + alignment slack
 
 // A neighbour-sum pass over a full 8192-double tile (the strided pass): the tile
-// of x arrives by bulk copies (one per run of 2^cp contiguous doubles) while
-// every thread prefetches its 32 values of y (or of scale * E when first) into
-// registers, so each SM keeps > 100 KB of loads in flight; then the neighbour
-// sums over tile bits [act_lo, 13) are read from shared memory.
-__global__ void __launch_bounds__(kFsThreads, 2) fs_tile_kernel(const double* __restrict__ x, double* __restrict__ y,
+// of x arrives as ONE tensor-map box (runs of 2^cp contiguous doubles, 2^w of
+// them 2^h0 doubles apart) while every thread prefetches its 32 values of y (or
+// of scale * E when first) into registers, so each SM keeps > 100 KB of loads in
+// flight; then the neighbour sums over tile bits [act_lo, 13) are read from
+// shared memory. (One bulk copy per run was measured 3-5x slower per byte than
+// one box for runs of a few hundred bytes.)
+__global__ void __launch_bounds__(kFsThreads, 2) fs_tile_kernel(const CUtensorMap* __restrict__ xmap,
+                                                                double* __restrict__ y,
                                                                 const uint16_t* __restrict__ E, double scale, double g,
-                                                                int cp, int h0, int mb, int first, int act_lo,
-                                                                int* err) {
-  extern __shared__ __align__(128) double ft[];
+                                                                int cp, int h0, int mb, int md, int hd, int first,
+                                                                int act_lo, int* err) {
+  // the tensor copy's destination must sit on a 128-byte boundary: the dynamic
+  // area gets 128 bytes of slack (kFsTileSmem) and the tile is aligned here
+  extern __shared__ __align__(128) unsigned char fs_raw[];
+  double* ft = reinterpret_cast<double*>(fs_raw + ((128u - (smem_addr(fs_raw) & 127u)) & 127u));
   __shared__ __align__(8) uint64_t bar;
   const uint32_t tid = threadIdx.x, tile = blockIdx.x;
+  if ((smem_addr(ft) & 127u) != 0u) {  // cannot happen after the alignment above; never issue a misaligned copy
+    if (tid == 0) atomicCAS(err, 0, DEV_BAD_LAUNCH);
+    return;
+  }
   const int w = kFsTileBits - cp;
-  const uint64_t mid = tile & ((1u << mb) - 1u), hi = tile >> mb;
-  const uint64_t base = (mid << cp) | (hi << (h0 + w));
+  const uint32_t mid = tile & ((1u << mb) - 1u), hi = tile >> mb;
+  const uint64_t base = ((uint64_t)mid << cp) | ((uint64_t)hi << (h0 + w));
   const uint32_t lo_mask = (1u << cp) - 1u;
   const uint32_t fb = smem_addr(&bar);
   if (tid == 0) {
     mbar_init(fb, 1);
     fence_barrier_init();
     mbar_arrive_expect_tx(fb, 8u << kFsTileBits);
+    tma_load_5d_hint(smem_addr(ft), xmap, tile_coord(0, md, (int)mid, hd, (int)hi),
+                     tile_coord(1, md, (int)mid, hd, (int)hi), tile_coord(2, md, (int)mid, hd, (int)hi),
+                     tile_coord(3, md, (int)mid, hd, (int)hi), tile_coord(4, md, (int)mid, hd, (int)hi), fb,
+                     policy_evict_first());
   }
+  // no thread may poll the barrier before thread 0 has initialised it
   __syncthreads();
-  const uint32_t rows = 1u << w, row_bytes = 8u << cp;
-  for (uint32_t r = tid; r < rows; r += kFsThreads)
-    bulk_load(smem_addr(ft + ((size_t)r << cp)), x + (base | ((uint64_t)r << h0)), row_bytes, fb);
   double pre[kFsPer];
 #pragma unroll
   for (int k = 0; k < kFsPer; ++k) {
