@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
     ap.add_argument("--engine-mode", type=int, default=None,
-                    help="0 persistent, 1 one launch per pass, 2 A1 launch + fused strided launch")
+                    help="0 persistent, 1 one launch per pass, 2 A1 launch + fused strided launch, "
+                         "3 the same with the fused strided pass in two self-served groups")
     ap.add_argument("--workload", choices=["large", "batched", "adjoint", "matvec"], default="large",
                     help="large: the N=28 headline; batched: 512 instances (64 traps x 8 g), N in {16,18,20,22}")
     ap.add_argument("--slab-lag", type=int, default=None)

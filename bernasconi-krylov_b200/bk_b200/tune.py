@@ -5,7 +5,8 @@ Knobs (engine options, include/bk_engine.h):
   engine_mode  0 = persistent dataflow kernel (every step in one launch, A1 tiles
                handed to S2 through L2), 1 = one grid launch per pass, 2 = the
                A1 pass as a grid launch and both strided passes in one
-               persistent launch (S3 re-reads S2's slabs from L2);
+               persistent launch (S3 re-reads S2's slabs from L2), 3 = mode 2
+               with the fused launch served by two self-loading groups;
   slab_lag     persistent engines: slabs between a slab's A1 and S2 tasks (mode
                0), or between a slab's S2 and S3 tasks (mode 2);
   split_w2     qubits of the S2 pass (the rest go to S3), 0 = engine default;
@@ -88,12 +89,13 @@ def candidates(n, precision):
             for wide in wides:
                 for lag in (1, 2, 3):
                     out.append(dict(engine_mode=2, slab_lag=lag, split_w2=w, e_source=0, a1_wide=wide))
+                out.append(dict(engine_mode=3, slab_lag=2, split_w2=w, e_source=0, a1_wide=wide))
     fused(rest, widths, (0, 1))
     if 1 <= rest9 <= 18:
         fused(rest9, [0] + [w for w in (d9 - 1, d9 + 1) if 3 <= w <= 9 and w <= rest9 and rest9 - w <= 9], (2, 3))
     # complex64: the full phase table with every per-pass candidate whose A1 kernel takes it (1-3)
     if precision == BK_C64:
-        out += [dict(c, phase_table=1) for c in list(out) if c["engine_mode"] in (1, 2)]
+        out += [dict(c, phase_table=1) for c in list(out) if c["engine_mode"] in (1, 2, 3)]
     # E recomputed in the pass, on the default split of both schedules
     out.append(dict(engine_mode=1, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))
     out.append(dict(engine_mode=0, slab_lag=3, split_w2=0, e_source=1, a1_wide=0))

@@ -764,7 +764,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   std::vector<unsigned long long> tasks23;
   uint32_t slabs23 = 0, per_slab23 = 0;
   S23Program prog23{};
-  if (grid_mode && c->engine_mode == 2 && w3 > 0) {
+  if (grid_mode && (c->engine_mode == 2 || c->engine_mode == 3) && w3 > 0) {
     SlabMap sm{kElemBits - w2, kElemBits - w3, 0, 0};
     sm.cpm = std::max(sm.cp2, sm.cp3);
     sm.bits = std::max(0, a1_bits - sm.cpm);
@@ -867,7 +867,7 @@ int persist_prepare(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, dou
   D.e_recompute = c->e_recompute;
   D.a1_bits = a1_bits;
   D.map_a1s = d_maps + 4;
-  D.a1_evict_first = (grid_mode && c->engine_mode == 2) ? 1 : 0;
+  D.a1_evict_first = (grid_mode && (c->engine_mode == 2 || c->engine_mode == 3)) ? 1 : 0;
   D.map_e_half = d_maps + 5;
 
   cudaStream_t st = c->stream;
@@ -970,13 +970,15 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
   const uint32_t n_a1 = run.n_a1, n_s2 = run.n_s2, n_s3 = run.n_s3;
   const InstDesc<R> D = run.D;
 
-  if (c->engine_mode == 1 || c->engine_mode == 2) {
+  if (c->engine_mode == 1 || c->engine_mode == 2 || c->engine_mode == 3) {
     // one grid launch per pass: A1, S2, S3 per step, measurement tiles at the end;
     // mode 2 runs S2 + S3 as one fused launch (S3 reads S2's slabs from L2)
     const bool fused23 = run.n_tasks23 > 0;
     S23Program P23 = run.prog23;
+    const bool self_served = c->engine_mode == 3;  // the fused strided pass without a producer warp
     if (fused23) {
       BK_TRY(allow_smem(c, reinterpret_cast<const void*>(s23_kernel<R>), kS23Smem));
+      BK_TRY(allow_smem(c, reinterpret_cast<const void*>(s23g_kernel<R>), kS23gSmem));
       P23.slab_done = run.ctr23;
       P23.next = run.ctr23 + run.slabs23;
       P23.ctas_done = run.ctr23 + run.slabs23 + 1;
@@ -1025,7 +1027,10 @@ int evolve_persist(bk_ctx* c, const bk_evolve_params* p, const Schedule& S, doub
       if (fused23) {
         BK_TRY(ev_begin(c, "tile_s23", &ev));
         P23.step = (uint32_t)k;
-        s23_kernel<R><<<c->num_sms, kS23Threads, kS23Smem, st>>>(D, P23);
+        if (self_served)
+          s23g_kernel<R><<<c->num_sms, kS23gThreads, kS23gSmem, st>>>(D, P23);
+        else
+          s23_kernel<R><<<c->num_sms, kS23Threads, kS23Smem, st>>>(D, P23);
         BK_CUDA(c, cudaGetLastError());
         BK_TRY(ev_end(c, ev));
         continue;
@@ -2198,7 +2203,7 @@ int bk_set_option(bk_ctx* c, int option, int64_t value) {
   if (!c) return BK_ERR_INVALID;
   switch (option) {
     case BK_OPT_ENGINE_MODE:
-      if (value < 0 || value > 2) return fail(c, BK_ERR_INVALID, "engine mode %lld", (long long)value);
+      if (value < 0 || value > 3) return fail(c, BK_ERR_INVALID, "engine mode %lld", (long long)value);
       c->engine_mode = (int)value;
       return BK_OK;
     case BK_OPT_SLAB_LAG:

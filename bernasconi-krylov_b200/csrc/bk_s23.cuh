@@ -272,4 +272,172 @@ __global__ void __launch_bounds__(kS23Threads, 1)
   if (tg == 0 && pending != kNone) red_release_add(P.slab_done + pending, 1u);
 }
 
+// ---------------------------------------------------------------------------
+// Fused strided pass without a producer warp (engine mode 3): two compute
+// groups of 8 warps per CTA (512 threads, so the tile code keeps 128 registers),
+// each serving itself from a private 64 KB stage. A group's leader claims its
+// next task one task ahead (the atomic's latency hides behind a tile), issues
+// the task's load into the group's stage as soon as the current tile's last
+// shared-memory read is done, and releases an S3 tile's slab counter at the
+// next such point (the stores have had a tile's compute to drain). A group never
+// waits on a slab counter while it holds an unfinished or unreleased task: when
+// the next task's slab is not complete at the stage-free point, its load is
+// deferred to the end of the current task, after the release. Claims are global
+// and in order, so the smallest unfinished task always has its dependencies
+// released and its group free: no deadlock. Same tile arithmetic as s23_kernel
+// (bit-identical results); every wait is bounded.
+// ---------------------------------------------------------------------------
+constexpr int kS23gThreads = 2 * kComputeThreads;  // 512
+
+// true in every thread of the 256-thread group (named barrier `id`) when any of them passes true
+__device__ __forceinline__ bool group_any(uint32_t id, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{ .reg .pred p, q; setp.ne.u32 p, %1, 0; bar.red.or.pred q, %2, 256, p; selp.u32 %0, 1, 0, q; }"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id)
+      : "memory");
+  return r != 0u;
+}
+__device__ __forceinline__ void fence_proxy_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+constexpr int kS23gSmem = 2 * kStageTileBytes;      // 128 KB
+
+template <class R>
+__global__ void __launch_bounds__(kS23gThreads, 1)
+    s23g_kernel(const __grid_constant__ InstDesc<R> D, const __grid_constant__ S23Program P) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full_bar[2];
+  __shared__ uint32_t s_task[2];  // the group's current claim index, published by its leader
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t grp = warp >> 3, tg = tid & 255u;
+  const bool leader = (tg == 0u);
+  const GroupSync sy{1u + grp};
+  unsigned char* stage = smem + (size_t)grp * kStageTileBytes;
+  const uint32_t fb = smem_addr(&full_bar[grp]);
+  const uint32_t target = (1u << P.lb) * (P.step + 1u);
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  // leader state
+  uint32_t pending = kNone;  // slab whose counter this group still owes a release
+  uint32_t ok_slab = kNone;  // slab seen complete
+  uint32_t ahead = 0u;       // the claim after the current one (issued one task early)
+  bool armed = false;        // a load is in flight into the stage
+  auto claim = [&]() -> uint32_t { return s23_aborted(P) ? P.n_tasks : atomicAdd(P.next, 1u); };
+  // leader: the slab of an S2 task complete (polls once if `block` is false)
+  auto slab_ready = [&](const S23Task& t, bool block) -> int {
+    if (t.kind != S23_S2 || t.slab == ok_slab) return 1;
+    const unsigned int* ctr = P.slab_done + t.slab;
+    uint32_t polls = 0;
+    while (ld_acquire(ctr) < target) {
+      if (!block) return 0;
+      if (++polls > P.poll_limit) {
+        s23_raise(P, DEV_TIMEOUT);
+        return -1;
+      }
+      if ((polls & 63u) == 0u && s23_aborted(P)) return -1;
+      __nanosleep(64);
+    }
+    fence_proxy_async_global();  // the TMA reads what the counter released
+    ok_slab = t.slab;
+    return 1;
+  };
+  auto issue = [&](const S23Task& t) {
+    fence_proxy_async_shared();  // the group's generic-proxy accesses of the stage precede the TMA's writes
+    StageMeta m;
+    m.kind = (t.kind == S23_S2) ? TASK_S2 : TASK_S3;
+    m.inst = 0;
+    m.tile = t.tile;
+    m.step = P.step;
+    issue_task_load(D, m, stage, fb);
+    armed = true;
+  };
+  if (tid == 0) {
+    mbar_init(smem_addr(&full_bar[0]), 1);
+    mbar_init(smem_addr(&full_bar[1]), 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (leader) {
+    uint32_t first = claim();
+    ahead = claim();
+    if (first < P.n_tasks) {
+      const S23Task t = s23_decode(P, first);
+      const int r = slab_ready(t, true);
+      if (r > 0) issue(t);
+      else first = P.n_tasks;
+    }
+    s_task[grp] = first;
+  }
+  sy.sync();
+  const R tn = D.tan[P.step];
+  uint32_t parity = 0;
+  for (;;) {
+    const uint32_t cur = s_task[grp];
+    if (cur >= P.n_tasks) break;
+    const bool landed = s23_wait(fb, parity, P);
+    if (group_any(1u + grp, !landed)) break;  // the whole group leaves together
+    parity ^= 1u;
+    if (leader) armed = false;
+    const S23Task task = s23_decode(P, cur);
+    bool deferred = false;
+    uint32_t nxt = P.n_tasks;
+    auto stage_free = [&]() {
+      if (!leader) return;
+      // the stage is free: the next task's load goes out now unless its slab is not complete yet
+      nxt = ahead;
+      ahead = (nxt < P.n_tasks) ? claim() : P.n_tasks;
+      if (nxt < P.n_tasks) {
+        const S23Task t = s23_decode(P, nxt);
+        if (slab_ready(t, false) > 0) issue(t);
+        else deferred = true;
+      }
+      if (pending != kNone) {
+        red_release_add(P.slab_done + pending, 1u);
+        pending = kNone;
+      }
+    };
+    const bool s2 = (task.kind == S23_S2);
+    const int w = s2 ? D.w2 : D.w3;
+    const int mb = s2 ? D.s2_mid_bits : D.s3_mid_bits;
+    const uint32_t h0 = s2 ? (uint32_t)D.a1_bits : (uint32_t)(D.a1_bits + D.w2);
+    const uint32_t cp = (uint32_t)(kElemBits - w);
+    const uint32_t mid = task.tile & ((1u << mb) - 1u), hi = task.tile >> mb;
+    const uint32_t tile_base = (mid << cp) | (hi << (h0 + (uint32_t)w));
+    process_s_dispatch<R>(w, stage, D.state, tile_base, h0, tn, stage_free, tg, sy,
+                          s2 ? policy_evict_first() : policy_evict_last());
+    if (!s2) {
+      sy.sync();  // every store of the group's tile precedes the (deferred) release
+      if (leader) pending = task.slab;
+    }
+    if (leader) {
+      if (deferred) {
+        // nothing of this group is unfinished or unreleased while it waits for the slab
+        if (pending != kNone) {
+          red_release_add(P.slab_done + pending, 1u);
+          pending = kNone;
+        }
+        const int r = slab_ready(s23_decode(P, nxt), true);
+        if (r > 0) issue(s23_decode(P, nxt));
+        else nxt = P.n_tasks;
+      }
+      s_task[grp] = nxt;
+    }
+    sy.sync();  // publishes the next claim (and orders this tile's reads of s_task before the write)
+  }
+  if (leader) {
+    if (pending != kNone) red_release_add(P.slab_done + pending, 1u);
+    if (armed) mbar_wait_bounded(fb, parity, P.err);  // a load in flight lands before the CTA leaves
+  }
+  __syncthreads();
+  if (tid == 0) {
+    // the last CTA out resets the claim counter for the next launch
+    __threadfence();
+    if (atomicAdd(P.ctas_done, 1u) == gridDim.x - 1u) {
+      *P.next = 0u;
+      *P.ctas_done = 0u;
+    }
+  }
+}
+
 }  // namespace bk

@@ -274,7 +274,9 @@ int bk_d_min(bk_ctx* ctx, int n, uint64_t bits, int64_t target, int max_d, int* 
  *       2 = a grid launch for the A1 pass and ONE persistent launch for both
  *       strided passes (S3 re-reads each slab S2 wrote from L2, so the strided
  *       part of a step crosses HBM once; sizes with a single strided pass run
- *       as mode 1);
+ *       as mode 1), 3 = mode 2 with the fused strided launch served by two
+ *       compute groups that load their own tiles (no producer warp); results
+ *       bit-identical to mode 2;
  *   BK_OPT_SLAB_LAG: persistent engine, slabs between A1 and S2 of a slab (>= 1);
  *   BK_OPT_SPLIT_W2: qubits of the S2 pass (1..9; the rest go to S3, at most 9),
  *       0 = the engine's default split; a width that does not fit a size is ignored;

@@ -120,3 +120,25 @@ def test_half_tile_warp_local_a1_equals_full_tile(eng, n, precision, mode):
     assert np.array_equal(s2, s3)
     assert np.max(np.abs(p2 - p3)) <= 1e-14 and np.max(np.abs(d2 - d3)) <= 1e-13 * n
     assert np.max(np.abs(n2 - n3)) <= 1e-14
+
+
+@pytest.mark.parametrize("n,precision", [(18, bk.BK_C64), (24, bk.BK_C64), (27, bk.BK_C64), (22, bk.BK_C128)])
+@pytest.mark.parametrize("lag", [1, 2])
+def test_self_served_groups_equal_producer_schedule(eng, n, precision, lag):
+    """Engine mode 3 (two compute groups claiming and loading their own tiles,
+    no producer warp) runs the same tiles in the same per-slab order as mode 2:
+    identical series and state."""
+    bits, e0 = bk.select_trap(n, 42, 300, 0.05)
+    meas = list(range(0, 25, 4))
+    out = {}
+    try:
+        for mode in (2, 3):
+            eng.set_option("engine_mode", mode)
+            eng.set_option("slab_lag", lag)
+            out[mode] = eng.evolve(n, bits, 0.35, 0.02, 24, measure=meas, e0=e0, precision=precision) + \
+                (eng.export_state(n),)
+    finally:
+        eng.set_option("engine_mode", 0)
+        eng.set_option("slab_lag", 3)
+    for a, b in zip(out[2], out[3]):
+        assert np.array_equal(a, b), (n, lag)

@@ -7,7 +7,8 @@ from bk_b200 import tune
 
 def test_candidates_cover_modes_lags_and_valid_splits():
     c = tune.candidates(28, bk.BK_C64)  # 27 element bits: A1 12 + 15 strided, default S2 width 8
-    assert {x["engine_mode"] for x in c} == {0, 1, 2}
+    assert {x["engine_mode"] for x in c} == {0, 1, 2, 3}
+    assert {x.get("phase_table", 0) for x in c if x["engine_mode"] in (1, 2, 3)} == {0, 1}
     assert {x["split_w2"] for x in c} == {0, 7, 9}
     assert {x["slab_lag"] for x in c if x["engine_mode"] == 0} == {1, 2, 3, 4, 6}
     assert {x["slab_lag"] for x in c if x["engine_mode"] == 2} == {1, 2, 3}
@@ -21,9 +22,11 @@ def test_candidates_cover_modes_lags_and_valid_splits():
             rest = np_ - (9 if x["a1_wide"] in (2, 3) else tune.ELEM_BITS)
             w = x["split_w2"] or tune.default_w2(rest)
             assert 1 <= w <= 9 and w <= rest and rest - w <= 9
-            assert x["a1_wide"] not in (2, 3) or (w >= 3 and x["engine_mode"] in (1, 2) and rest <= 18)
+            assert x["a1_wide"] not in (2, 3) or (w >= 3 and x["engine_mode"] in (1, 2, 3) and rest <= 18)
             # the fused strided pass is only tried where a third pass is left to fuse
-            assert x["engine_mode"] != 2 or rest - w >= 1
+            assert x["engine_mode"] not in (2, 3) or rest - w >= 1
+            # the full phase table: complex64 per-pass schedules only
+            assert not x.get("phase_table") or (prec == bk.BK_C64 and x["engine_mode"] in (1, 2, 3))
 
 
 def test_cache_round_trip(tmp_path):
