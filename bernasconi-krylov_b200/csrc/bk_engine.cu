@@ -2907,7 +2907,8 @@ int fs_err_check(bk_ctx* c) {
   int e = 0;
   BK_CUDA(c, cudaMemcpyAsync(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   BK_CUDA(c, cudaStreamSynchronize(c->stream));
-  if (e != 0) return fail(c, BK_ERR_TIMEOUT, "fullspace matvec: a bounded device wait gave up (%d)", e);
+  if (e == DEV_TIMEOUT) return fail(c, BK_ERR_TIMEOUT, "fullspace matvec: a bounded device wait gave up");
+  if (e != 0) return fail(c, BK_ERR_CUDA, "fullspace matvec: a kernel refused its launch geometry (%d)", e);
   return BK_OK;
 }
 
