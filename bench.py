@@ -699,7 +699,12 @@ def main():
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": abytes, "avg_launch_ms": dms / dl,
-                         "traffic": traffic},
+                         "traffic": traffic,
+                         # the whole Trotter step against the two-round-trip model (4 S bytes per amplitude-step)
+                         "step": {"algorithmic_bytes": 4.0 * S * float(1 << n),
+                                  "ms": 1e3 * dev_s_max / (a.steps * T),
+                                  "achieved": 4.0 * S * float(1 << n) / (dev_s_max / (a.steps * T)) / 1e9,
+                                  "frac": 4.0 * S * float(1 << n) / (dev_s_max / (a.steps * T)) / 1e9 / peak}},
             "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 3)} for k, v in timing.items()},
             "kernel_table": f"{table_steps} bench steps with CUDA events around every launch, after the timed "
                             "region (the timed region runs without them)",
